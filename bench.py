@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark of the DMM integrator hot path: clause-updates/s.
+
+Workload (one GPU): planted random 3-SAT, n = 100,000 variables, m = 800,000 clauses
+(r = 8; the number of literals agreeing with the planted assignment is 3 with probability
+0.08 and 1 or 2 with probability 0.46 each), FP32 production state, initial state
+V ~ U[-1,1], Xs ~ U[0,1], Xl = 1.  Synthetic data: the reference's own n = 100,000
+instances are not available, so the project generator with these parameters stands in.
+
+A "step" is one accepted integration step (right-hand side of every clause, deterministic
+per-variable reduction, adaptive h, Euler update) of that instance.  `value` is
+m x steps / device time of the timed steps, with an L2 flush (256 MiB write) before every
+timed step so each step starts from HBM; `e2e` is the same metric through the C ABI from
+host buffers (create + state upload + steps + assignment readback).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one independent instance per GPU (replicas; no collective on
+the data path), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dynex-neuromorphic-chip_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+N_VARS, N_CLAUSES, P0, P1 = 100_000, 800_000, 0.08, 0.46
+INSTANCE_SEED, INIT_SEED = 1, 1001
+FLUSH_BYTES = 256 << 20
+METRIC = "clause-updates/s"
+WORKLOAD = "planted 3-SAT n=100000 m=800000 r=8 p0=0.08 (plain single instance, FP32)"
+E2E_STEPS = 64
+CPU_SAMPLE_STEPS = 60
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---- helpers ------------------------------------------------------------------------------
+
+class Clocks:
+    """nvidia-smi samples (every 200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.25)
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per launch of the clause kernel at this workload, from the committed
+    ncu summary (profiles/k_clause_n100k.md, line `traffic_bytes_per_launch: X`)."""
+    p = os.path.join(ROOT, "profiles", "k_clause_n100k.md")
+    try:
+        with open(p) as f:
+            m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def make_instance(rank: int):
+    import dmm_b200 as dmm
+
+    form, planted = dmm.generate_planted(N_VARS, N_CLAUSES, P0, P1, seed=INSTANCE_SEED + rank)
+    x0 = dmm.initial_state_uniform(form, INIT_SEED + rank)
+    return form, x0
+
+
+# ---- reference arm (CPU) ------------------------------------------------------------------
+
+def _ref_worker(args):
+    rank, steps, warmup = args
+    import numpy as np  # noqa: F401
+
+    from oracle.oracle import Reference
+
+    form, x0 = make_instance(rank)
+    ref = Reference(form.n, form.m, form.lits, form.clause_off)
+    if warmup:
+        ref.run(x0, warmup)
+    t0 = time.perf_counter()
+    r = ref.run(x0, steps)
+    dt = time.perf_counter() - t0
+    return r["steps"], dt
+
+
+def cpu_reference(steps: int, warmup: int, procs: int):
+    """The unmodified reference integrator (oracle/_ref, dynex.cc's own right-hand side and
+    Euler step) on `procs` host processes at once, each on its own instance."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [(r, steps, warmup) for r in range(procs)])
+        wall = time.perf_counter() - t0
+    done = sum(s for s, _ in res)
+    t = max(d for _, d in res)
+    return N_CLAUSES * done / t, {"procs": procs, "steps_each": steps, "timed_s": t,
+                                  "wall_s": wall}
+
+
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = max(1, os.cpu_count() or 1)
+    steps = max(1, a.steps // 4)
+    t_all = []
+    for _ in range(a.warmup if a.warmup < 1 else 1):
+        pass
+    value, info = cpu_reference(steps, 0, procs)
+    t_all.append(info)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "clause-updates/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000.0 * info["timed_s"] / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("FP32", "FP64 reference CPU"),
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "clause-updates/s", "cores": procs,
+                         "kind": "reference",
+                         "sample": f"{procs} processes x {steps} steps of the n=100000 "
+                                   "instance (each process its own seed)"},
+        "e2e": {"value": value, "unit": "clause-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ------------------------------------------------------------------------------
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import numpy as np
+    import torch
+
+    import dmm_b200 as dmm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    form, x0 = make_instance(rank)
+    n, m = form.n, form.m
+    K, W = a.steps, max(3, a.warmup)
+    inst = dmm.Instance(form, precision="fp32", device=local)
+    init_seed = INIT_SEED + rank
+    for attempt in range(4):
+        inst.set_state(x0)
+        inst.profile(W, FLUSH_BYTES)  # warm-up: same launches as the timed region
+        barrier()
+        s0 = inst.report().steps
+        with Clocks(local) as clk:
+            clause_ms, var_ms = inst.profile(K, FLUSH_BYTES)
+        barrier()
+        steps_done = inst.report().steps - s0
+        if steps_done == K:
+            break
+        # solved inside the timed region: the remaining steps would be no-ops; restart
+        init_seed += 1000
+        x0 = dmm.initial_state_uniform(form, init_seed)
+    clocks = clk.summary()
+    step_ms = clause_ms + var_ms
+    t_max = max_over_ranks(step_ms)
+    total_updates = sum_over_ranks(m * steps_done)
+    value = total_updates / (t_max / 1000.0)
+
+    # resident: the solver's own launch path (CUDA graphs, no flush; the 3.5e7-byte working
+    # set of this instance stays in the 126 MB L2 between steps)
+    inst.set_state(x0)
+    inst.time_steps(W)
+    s0 = inst.report().steps
+    res_ms = inst.time_steps(K)
+    res_steps = inst.report().steps - s0
+    resident_value = sum_over_ranks(m * res_steps) / (max_over_ranks(res_ms) / 1000.0)
+
+    # end to end through the C ABI from pinned host buffers
+    lits_p = torch.from_numpy(form.lits).pin_memory()
+    off_p = torch.from_numpy(form.clause_off).pin_memory()
+    x0_p = torch.from_numpy(x0).pin_memory()
+    pform = dmm.Formula(n, m, lits_p.numpy(), off_p.numpy(), form.max_occurrence)
+    e2e_times, e2e_steps = [], []
+    for it in range(3 + 2):
+        barrier()
+        t0 = time.perf_counter()
+        with dmm.Instance(pform, precision="fp32", device=local) as e:
+            e.set_state(x0_p.numpy())
+            r = e.step(E2E_STEPS)
+            _, post = e.assignment(pre=False)
+        dt = time.perf_counter() - t0
+        if it >= 2:
+            e2e_times.append(dt)
+            e2e_steps.append(r.steps)
+    e2e_t = max_over_ranks(statistics.median(e2e_times))
+    e2e_value = sum_over_ranks(m * statistics.median(e2e_steps)) / e2e_t
+    h2d = form.lits.nbytes + form.clause_off.nbytes + x0.nbytes
+    d2h = n + 56
+
+    peak, peak_kind = peaks()
+    algo_bytes = 28 * m + 4 * n  # clause kernel: literals 12m, Xs/Xl read+write 16m, V 4n
+    clause_launch_ms = max_over_ranks(clause_ms / K)
+    achieved = algo_bytes / (clause_launch_ms / 1000.0) / 1e9
+    traffic = profiled_traffic()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, info = cpu_reference(CPU_SAMPLE_STEPS, 0, 1)
+        cpu = {"value": v, "unit": "clause-updates/s", "cores": 1, "kind": "reference",
+               "sample": f"{CPU_SAMPLE_STEPS} steps of the same instance and initial state, "
+                         "reference dynex.cc right-hand side + Euler step, 1 thread"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "clause-updates/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": t_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "m": m, "per_gpu_instances": 1,
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": f"replicas x{world}", "tuning": inst.tuning},
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": "clause-updates/s",
+                    "h2d_bytes_per_step": h2d / E2E_STEPS, "d2h_bytes_per_step": d2h / E2E_STEPS,
+                    "path": f"dmm_instance_create + set_state + {E2E_STEPS} steps + assignment "
+                            "readback, pinned host buffers"},
+            "gpu_launches": 2 * K,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_clause", "peak_kind": peak_kind,
+                         "algo_bytes_per_launch": algo_bytes},
+            "kernels_ms_per_step": {"k_clause": clause_ms / K, "k_var": var_ms / K},
+            "resident": {"value": resident_value, "unit": "clause-updates/s",
+                         "ms_per_step": res_ms / max(1, res_steps),
+                         "note": "CUDA-graph launches, no L2 flush (solver's own mode)"},
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    inst.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

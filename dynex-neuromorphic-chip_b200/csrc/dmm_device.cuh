@@ -1,0 +1,114 @@
+// Device-side data layout and arithmetic of the DMM integrator (sm_100a).
+//
+// A *pack* holds one or many formulas in shared device arrays.  Every formula (an
+// "instance") owns a contiguous range in three index spaces:
+//   variables [var0, var0+n)   : candidate voltages, unit pins, CSR ends
+//   clauses   [cls0, cls0+m)   : Xs, Xl, C of the last right-hand side, per-clause alpha
+//   slots     [slot0, slot0+L) : one per literal occurrence: literal, contribution u,
+//                                and (in variable order) the CSR list of slots
+// The work of one step is cut into clause tiles and variable tiles that never straddle
+// instances, so an instance's arithmetic is identical alone or packed with others.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dmm {
+
+constexpr int kMaxK = 25;          // longest clause (MAX_LITS_SYSTEM, dynex.cc:69)
+constexpr int kThreads = 256;      // block size of every tile kernel (fixed: reductions
+                                   // over a block are part of the result definition)
+constexpr int kTrials = 4;         // adaptive trials h = 1/8, 1/16, 1/32, 1/64
+
+// Read-only description of one instance.
+struct InstDesc {
+  int32_t n, m;
+  int64_t var0, cls0, slot0;
+  int32_t nslots;
+  int32_t k3;            // every clause has exactly 3 literals: slot of clause c is 3c
+  int32_t has_alpha_cm;  // per-clause alpha array present
+  int32_t max_steps;     // accepted-step cap, <= 0: none
+  int32_t ctile0, nctile, vtile0, nvtile;
+  double alpha, beta, gamma, delta, eps, zeta, xl_max;
+};
+
+// Mutable integration state of one instance (written by the finalize step).
+struct InstCtrl {
+  int32_t done;         // dmm_run_status; 0 while running
+  int32_t step;         // accepted steps (reference stepcounter)
+  int32_t set;          // candidate set holding V(step)
+  int32_t kcur;         // trial slot of V(step) in that set
+  int32_t pending;      // Xs/Xl Euler update of the previous step not yet applied
+  int32_t loc;          // loc of the last right-hand side
+  int32_t best_loc;
+  int32_t solved_step;  // step at which the solving right-hand side ran, -1
+  int32_t sol_set, sol_k;
+  int32_t vfail;        // strict-sign failures of the last right-hand side
+  int32_t pad0;
+  double t;             // simulated time
+  double h_state;       // h of the pending Xs/Xl update
+  double energy;        // energy of the last right-hand side
+  double solved_t;
+  double best_t;
+  // per-step accumulators, zeroed by the finalize step
+  int32_t acc_loc, acc_vfail, acc_kmax, vtiles_done;
+};
+
+struct Tile {
+  int32_t inst;
+  int32_t begin;  // local clause / variable index
+  int32_t count;
+  int32_t pad;
+};
+
+template <class T>
+struct PackView {
+  T* Xs;
+  T* Xl;
+  T* Cp;                    // C_m of the last right-hand side (for the deferred update)
+  const T* alpha_cm;        // per-clause alpha (may be null)
+  const int32_t* coff;      // general layout: local slot offset of each clause
+  const int32_t* lit;       // local signed literal of each slot (1-based variable)
+  T* u;                     // contribution of each slot
+  const int32_t* vslot;     // variable-ordered slot list (local slot indices)
+  const int32_t* vend;      // inclusive end of each variable's slot list (local)
+  T* cand;                  // candidates: cand[(set*4 + k) * var_cap + v]
+  int64_t var_cap;
+  const int8_t* unit;       // +1/-1 pin of unit-clause variables, else 0
+  double* epart;            // energy partial of each clause tile
+  const InstDesc* inst;
+  InstCtrl* ctrl;
+  const Tile* ctiles;
+  const Tile* vtiles;
+  const int32_t* ntiles;    // [0] clause tiles, [1] variable tiles
+  int32_t* queue;           // [0] clause-tile counter, [1] variable-tile counter
+  int32_t* active;          // instances still running
+  int32_t* ring;            // finished instances (ring buffer)
+  int32_t* ring_tail;
+  int32_t ring_cap;
+};
+
+// ---- exactly rounded arithmetic (no FMA contraction: the reference has none) ----------
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+template <class T>
+__device__ __forceinline__ T clampv(T x, T lo, T hi) {
+  x = (x < lo) ? lo : x;
+  return (x > hi) ? hi : x;
+}
+
+template <class T>
+__device__ __forceinline__ T inf_val();
+template <>
+__device__ __forceinline__ float inf_val<float>() { return __int_as_float(0x7f800000); }
+template <>
+__device__ __forceinline__ double inf_val<double>() {
+  return __longlong_as_double(0x7ff0000000000000ll);
+}
+
+}  // namespace dmm

@@ -1,0 +1,837 @@
+// Hot-path kernels of the DMM integrator for sm_100a.
+//
+// One accepted step of the reference integrator (dmm_generate_dxdt + the adaptive
+// dmm_dostep loop, dynex.cc:332-530, 301-327, 1389-1417) is two kernels:
+//
+//   k_clause  (per clause tile)   applies the previous step's Euler update to Xs/Xl
+//             (deferred, because the accepted h is only known after every variable is
+//             reduced), evaluates C_m, G, R and the per-literal contributions u, stores u
+//             per literal slot, and counts unsatisfied clauses (C_m >= 1/2) plus
+//             strict-sign failures with warp ballots; energy partial per tile in FP64.
+//   k_var     (per variable tile) reduces each variable's contributions over the
+//             variable->slot CSR in a fixed order without atomics, forms the four Euler
+//             candidates V + h*dV (h = 1/8 .. 1/64) with unit pin and clamps, and the
+//             first trial each variable accepts.  The last tile of an instance finalizes
+//             the step: accepted trial = max over variables, t += h, solved / limit.
+//
+// The four candidates replace the reference's retry loop: |clamp(V + h dV) - V| is
+// monotone in h, so the first h the reference accepts is the largest h every variable
+// accepts, i.e. trial max_v k_v (and when no trial passes, the reference keeps the 1/64
+// state and advances t by 1/128, dynex.cc:1401-1411).
+//
+// Results never depend on the launch shape: clause work is per clause, per-variable sums
+// use one canonical order for every lane grouping, tiles never straddle instances, and
+// every cross-block combination is an integer atomic or a fixed-order reduction.
+#pragma once
+
+#include "dmm_device.cuh"
+
+namespace dmm {
+
+// ---- block reductions (fixed order: warp butterflies, then warp 0 over the warps) ---------
+
+__device__ __forceinline__ int warp_sum_i(int v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_max_i(int v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum of a double over the block; valid in thread 0.  `red` holds kThreads/32 doubles.
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  v = warp_sum_d(v);
+  const int w = threadIdx.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = (threadIdx.x < kThreads / 32) ? red[threadIdx.x] : 0.0;
+    r = warp_sum_d(r);
+  }
+  return r;
+}
+
+// ---- clause right-hand side ------------------------------------------------------------
+
+template <class T>
+struct ClauseConsts {
+  T beta, gamma, delta, eps, zeta, xlmax, alpha, h;
+};
+
+template <class T>
+__device__ __forceinline__ ClauseConsts<T> make_consts(const InstDesc& I, double h) {
+  ClauseConsts<T> c;
+  c.beta = T(I.beta);
+  c.gamma = T(I.gamma);
+  c.delta = T(I.delta);
+  c.eps = T(I.eps);
+  c.zeta = T(I.zeta);
+  c.xlmax = T(I.xl_max);
+  c.alpha = T(I.alpha);
+  c.h = T(h);
+  return c;
+}
+
+// Deferred Euler update of one clause's memories: the reference computes
+// dXs = beta (Xs_c + eps)(C - gamma), dXl = alpha_m (C - delta) from the clamped reads
+// (dynex.cc:366-367, 503, 506) and then x + h dx with clamps (dynex.cc:313-322).
+template <class T>
+__device__ __forceinline__ void advance_memory(T& Xs, T& Xl, T Cp, T alpha_c,
+                                               const ClauseConsts<T>& k) {
+  const T one = T(1), zero = T(0);
+  const T xs_c = clampv(Xs, zero, one);
+  const T dxs = mul(mul(k.beta, add(xs_c, k.eps)), sub(Cp, k.gamma));
+  const T dxl = mul(alpha_c, sub(Cp, k.delta));
+  Xs = clampv(add(Xs, mul(k.h, dxs)), zero, one);
+  Xl = clampv(add(Xl, mul(k.h, dxl)), one, k.xlmax);
+}
+
+template <class T>
+__device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
+
+// 3-literal clause (dynex.cc:371-418).  v*: raw voltages.  Returns C_m.
+template <class T>
+__device__ __forceinline__ T clause3(int l0, int l1, int l2, T v0, T v1, T v2, T Xs, T Xl,
+                                     const ClauseConsts<T>& k, T& u0, T& u1, T& u2,
+                                     bool& strict_sat) {
+  const T one = T(1), half = T(0.5), zero = T(0);
+  strict_sat = (v0 > zero && l0 > 0) || (v0 < zero && l0 < 0) || (v1 > zero && l1 > 0) ||
+               (v1 < zero && l1 < 0) || (v2 > zero && l2 > 0) || (v2 < zero && l2 < 0);
+  const T c0 = clampv(v0, -one, one), c1 = clampv(v1, -one, one), c2 = clampv(v2, -one, one);
+  const T q0 = l0 > 0 ? one : -one, q1 = l1 > 0 ? one : -one, q2 = l2 > 0 ? one : -one;
+  const T a0 = sub(one, mul(q0, c0)), a1 = sub(one, mul(q1, c1)), a2 = sub(one, mul(q2, c2));
+  const T m12 = tmin(a1, a2), m02 = tmin(a0, a2), m01 = tmin(a0, a1);
+  const T C = mul(tmin(a0, m12), half);
+  const T xs = clampv(Xs, zero, one), xl = clampv(Xl, one, k.xlmax);
+  const T xlxs = mul(xl, xs);
+  const T rfac = mul(add(one, mul(k.zeta, xl)), sub(one, xs));
+  const T g0 = mul(mul(q0, m12), half), g1 = mul(mul(q1, m02), half),
+          g2 = mul(mul(q2, m01), half);
+  const T r0 = (C == mul(a0, half)) ? mul(sub(q0, c0), half) : zero;
+  const T r1 = (C == mul(a1, half)) ? mul(sub(q1, c1), half) : zero;
+  const T r2 = (C == mul(a2, half)) ? mul(sub(q2, c2), half) : zero;
+  u0 = add(mul(xlxs, g0), mul(rfac, r0));
+  u1 = add(mul(xlxs, g1), mul(rfac, r1));
+  u2 = add(mul(xlxs, g2), mul(rfac, r2));
+  return C;
+}
+
+// General clause of k literals (2-SAT dynex.cc:420-454 and k-SAT dynex.cc:457-494 compute
+// the same values as this loop; k = 1 runs no branch, C = 0; k = 0 leaves C = INT_MAX/2).
+template <class T>
+__device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int k,
+                                            const T* __restrict__ V, T Xs, T Xl,
+                                            const ClauseConsts<T>& kc, T* __restrict__ u,
+                                            bool& strict_sat) {
+  const T one = T(1), half = T(0.5), zero = T(0);
+  strict_sat = false;
+  if (k == 0) return mul(T(2147483647.0), half);
+  if (k == 1) {
+    const int l = __ldg(lit);
+    const T v = V[abs(l) - 1];
+    strict_sat = (v > zero && l > 0) || (v < zero && l < 0);
+    u[0] = zero;
+    return zero;
+  }
+  T a[kMaxK];
+  T mn = T(2147483647.0), mn2 = T(2147483647.0);
+  int arg = -1;
+  for (int j = 0; j < k; j++) {
+    const int l = __ldg(lit + j);
+    const T v = V[abs(l) - 1];
+    strict_sat |= (v > zero && l > 0) || (v < zero && l < 0);
+    const T q = l > 0 ? one : -one;
+    a[j] = sub(one, mul(q, clampv(v, -one, one)));
+    if (a[j] < mn) {
+      mn2 = mn;
+      mn = a[j];
+      arg = j;
+    } else if (a[j] < mn2) {
+      mn2 = a[j];
+    }
+  }
+  const T C = mul(mn, half);
+  const T xs = clampv(Xs, zero, one), xl = clampv(Xl, one, kc.xlmax);
+  const T xlxs = mul(xl, xs);
+  const T rfac = mul(add(one, mul(kc.zeta, xl)), sub(one, xs));
+  for (int j = 0; j < k; j++) {
+    const int l = __ldg(lit + j);
+    const T q = l > 0 ? one : -one;
+    const T c = clampv(V[abs(l) - 1], -one, one);
+    const T others = (j == arg) ? mn2 : mn;
+    const T g = mul(mul(q, others), half);
+    const T r = (C == mul(a[j], half)) ? mul(sub(q, c), half) : zero;
+    u[j] = add(mul(xlxs, g), mul(rfac, r));
+  }
+  return C;
+}
+
+struct TileSnap {
+  int32_t done, pending, set, kcur;
+  double h;
+};
+
+// Clause tiles.  Per tile: one InstDesc and one control snapshot in shared memory.
+template <class T, bool VEC>
+__global__ void __launch_bounds__(kThreads) k_clause(PackView<T> P) {
+  __shared__ InstDesc s_inst;
+  __shared__ TileSnap s_snap;
+  __shared__ Tile s_tile;
+  __shared__ int s_ti;
+  __shared__ double s_red[kThreads / 32];
+  __shared__ int s_cnt[2][kThreads / 32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) P.queue[1] = 0;  // variable-tile queue is idle
+  const int ntiles = P.ntiles[0];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int ti = atomicAdd(&P.queue[0], 1);
+      s_ti = ti;
+      if (ti < ntiles) {
+        s_tile = P.ctiles[ti];
+        s_inst = P.inst[s_tile.inst];
+        const InstCtrl* S = P.ctrl + s_tile.inst;
+        s_snap.done = S->done;
+        s_snap.pending = S->pending;
+        s_snap.set = S->set;
+        s_snap.kcur = S->kcur;
+        s_snap.h = S->h_state;
+      }
+    }
+    __syncthreads();
+    const int ti = s_ti;
+    if (ti >= ntiles) break;
+    if (s_snap.done == 0) {
+      const InstDesc& I = s_inst;
+      const ClauseConsts<T> kc = make_consts<T>(I, s_snap.h);
+      const bool pending = s_snap.pending != 0;
+      const T* __restrict__ V =
+          P.cand + (int64_t)(s_snap.set * kTrials + s_snap.kcur) * P.var_cap + I.var0;
+      T* __restrict__ Xs = P.Xs + I.cls0;
+      T* __restrict__ Xl = P.Xl + I.cls0;
+      T* __restrict__ Cp = P.Cp + I.cls0;
+      const T* __restrict__ acm = I.has_alpha_cm ? P.alpha_cm + I.cls0 : nullptr;
+      const int32_t* __restrict__ lit = P.lit + I.slot0;
+      T* __restrict__ u = P.u + I.slot0;
+      const int c_begin = s_tile.begin, c_end = s_tile.begin + s_tile.count;
+      int unsat = 0, vfail = 0;
+      double e = 0.0;
+      auto one_clause = [&](int c) {
+        T xs = Xs[c], xl = Xl[c];
+        const T al = acm ? acm[c] : kc.alpha;
+        if (pending) advance_memory(xs, xl, Cp[c], al, kc);
+        bool ss;
+        T C;
+        if (I.k3) {
+          const int l0 = __ldg(lit + 3 * c), l1 = __ldg(lit + 3 * c + 1),
+                    l2 = __ldg(lit + 3 * c + 2);
+          T u0, u1, u2;
+          C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1], xs, xl, kc,
+                      u0, u1, u2, ss);
+          u[3 * c] = u0;
+          u[3 * c + 1] = u1;
+          u[3 * c + 2] = u2;
+        } else {
+          const int s0 = P.coff[I.cls0 + c];
+          const int s1 = (c + 1 < I.m) ? P.coff[I.cls0 + c + 1] : I.nslots;
+          C = clause_general(lit + s0, s1 - s0, V, xs, xl, kc, u + s0, ss);
+        }
+        Xs[c] = xs;
+        Xl[c] = xl;
+        Cp[c] = C;
+        unsat += !(C < T(0.5));
+        vfail += !ss;
+        e += (double)C;
+      };
+      auto generic_loop = [&]() {
+        for (int c = c_begin + threadIdx.x; c < c_end; c += kThreads) one_clause(c);
+      };
+      if constexpr (!VEC) {
+        generic_loop();
+      } else if (!I.k3) {
+        generic_loop();
+      } else {
+        // 4 consecutive clauses per thread: 16-byte loads of 12 literals, Xs, Xl, C, and
+        // 16-byte stores of 12 contributions.
+        for (int g = c_begin + 4 * threadIdx.x; g < c_end; g += 4 * kThreads) {
+          if (g + 4 <= c_end) {
+            const int4* L4 = reinterpret_cast<const int4*>(lit + 3 * g);
+            const int4 A = __ldg(L4), B = __ldg(L4 + 1), Cc = __ldg(L4 + 2);
+            const int L[12] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w, Cc.x, Cc.y, Cc.z, Cc.w};
+            const float4 xs4 = *reinterpret_cast<const float4*>(Xs + g);
+            const float4 xl4 = *reinterpret_cast<const float4*>(Xl + g);
+            float4 cp4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (pending) cp4 = *reinterpret_cast<const float4*>(Cp + g);
+            float4 al4 = make_float4(kc.alpha, kc.alpha, kc.alpha, kc.alpha);
+            if (acm) al4 = *reinterpret_cast<const float4*>(acm + g);
+            float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w};
+            float xl[4] = {xl4.x, xl4.y, xl4.z, xl4.w};
+            const float cp[4] = {cp4.x, cp4.y, cp4.z, cp4.w};
+            const float al[4] = {al4.x, al4.y, al4.z, al4.w};
+            float uu[12], cc[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              if (pending) advance_memory(xs[i], xl[i], T(cp[i]), T(al[i]), kc);
+              bool ss;
+              const int l0 = L[3 * i], l1 = L[3 * i + 1], l2 = L[3 * i + 2];
+              T u0, u1, u2;
+              const T C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1],
+                                  T(xs[i]), T(xl[i]), kc, u0, u1, u2, ss);
+              uu[3 * i] = u0;
+              uu[3 * i + 1] = u1;
+              uu[3 * i + 2] = u2;
+              cc[i] = C;
+              unsat += !(C < T(0.5));
+              vfail += !ss;
+              e += (double)C;
+            }
+            float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
+            U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
+            U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
+            U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
+            *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
+            *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
+            *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+          } else {
+            for (int c = g; c < c_end; c++) one_clause(c);
+          }
+        }
+      }
+      // unsatisfied / strict-fail counts by ballot+popc, then over warps
+      const int w = threadIdx.x >> 5;
+      unsat = warp_sum_i(unsat);
+      vfail = warp_sum_i(vfail);
+      if ((threadIdx.x & 31) == 0) {
+        s_cnt[0][w] = unsat;
+        s_cnt[1][w] = vfail;
+      }
+      const double et = block_sum_d(e, s_red);
+      if (threadIdx.x == 0) {
+        int tu = 0, tv = 0;
+        for (int i = 0; i < kThreads / 32; i++) {
+          tu += s_cnt[0][i];
+          tv += s_cnt[1][i];
+        }
+        InstCtrl* S = P.ctrl + s_tile.inst;
+        if (tu) atomicAdd(&S->acc_loc, tu);
+        if (tv) atomicAdd(&S->acc_vfail, tv);
+        P.epart[ti] = et;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- per-variable reduction ---------------------------------------------------------------
+
+// Canonical FP32/FP64 sum of d contributions with G lanes per variable.  Virtual lane
+// vl in [0,32) accumulates entries j = vl, vl+32, ... in order; the 32 partials are then
+// combined by xor butterflies with offsets 16, 8, 4, 2, 1.  Lane `lane` of the group
+// holds virtual lanes lane + G*i; butterflies with offset >= G are lane-local, smaller
+// ones are shuffles.  Every G gives the same value.  All 32 lanes of the warp must call.
+template <class T, int G>
+__device__ __forceinline__ T tree_sum(const T* __restrict__ u, const int32_t* __restrict__ vs,
+                                      int d, int lane) {
+  constexpr int NV = 32 / G;
+  T p[NV];
+#pragma unroll
+  for (int i = 0; i < NV; i++) p[i] = T(0);
+  for (int base = 0; base < d; base += 32) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      const int j = base + lane + G * i;
+      if (j < d) p[i] = add(p[i], u[__ldg(vs + j)]);
+    }
+  }
+#pragma unroll
+  for (int off = 16; off >= G; off >>= 1) {
+    T q[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) q[i] = add(p[i], p[i ^ (off / G)]);
+#pragma unroll
+    for (int i = 0; i < NV; i++) p[i] = q[i];
+  }
+#pragma unroll
+  for (int off = G / 2; off >= 1; off >>= 1) p[0] = add(p[0], __shfl_xor_sync(0xffffffffu, p[0], off));
+  return p[0];
+}
+
+// Reference summation (dynex.cc:527-530): contributions sorted ascending, summed left to
+// right from +0.0 (zero contributions, which the reference skips, change no partial sum).
+// One warp per variable; d must be warp-uniform.  Bitonic sort in registers for d <= 32R.
+template <int R>
+__device__ __forceinline__ double sorted_sum_reg(const double* __restrict__ u,
+                                                 const int32_t* __restrict__ vs, int d,
+                                                 int lane) {
+  double a[R];
+  const double pinf = inf_val<double>();
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int j = r * 32 + lane;
+    a[r] = (j < d) ? u[__ldg(vs + j)] : pinf;
+  }
+  constexpr int N = 32 * R;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int jr = j / 32;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const int r2 = r ^ jr;
+          if (r2 > r) {
+            const int e = r * 32 + lane;
+            const bool up = (e & k) == 0;
+            const double x = a[r], y = a[r2];
+            const bool sw = up ? (y < x) : (x < y);
+            a[r] = sw ? y : x;
+            a[r2] = sw ? x : y;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const int e = r * 32 + lane;
+          const double o = __shfl_xor_sync(0xffffffffu, a[r], j);
+          const bool up = (e & k) == 0;
+          const bool lower = (e & j) == 0;
+          const bool take_min = (lower == up);
+          const double mn = (o < a[r]) ? o : a[r];
+          const double mx = (o < a[r]) ? a[r] : o;
+          a[r] = take_min ? mn : mx;
+        }
+      }
+    }
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    for (int l = 0; l < 32; l++) {
+      const double x = __shfl_sync(0xffffffffu, a[r], l);
+      if (r * 32 + l < d) acc = __dadd_rn(acc, x);
+    }
+  }
+  return acc;
+}
+
+// Long lists: repeated selection of the next (value, position) pair in lexicographic
+// order; O(d^2 / 32) loads, no scratch memory.
+__device__ __noinline__ double sorted_sum_select(const double* __restrict__ u,
+                                                 const int32_t* __restrict__ vs, int d,
+                                                 int lane) {
+  double acc = 0.0;
+  double lv = -inf_val<double>();
+  int li = -1;
+  for (int it = 0; it < d; it++) {
+    double bv = inf_val<double>();
+    int bi = 0x7fffffff;
+    for (int j = lane; j < d; j += 32) {
+      const double x = u[__ldg(vs + j)];
+      const bool after = (x > lv) || (x == lv && j > li);
+      const bool better = (x < bv) || (x == bv && j < bi);
+      if (after && better) {
+        bv = x;
+        bi = j;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov < bv || (ov == bv && oi < bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    acc = __dadd_rn(acc, bv);
+    lv = bv;
+    li = bi;
+  }
+  return acc;
+}
+
+__device__ __forceinline__ double sorted_sum(const double* __restrict__ u,
+                                             const int32_t* __restrict__ vs, int d, int lane) {
+  if (d <= 32) return sorted_sum_reg<1>(u, vs, d, lane);
+  if (d <= 64) return sorted_sum_reg<2>(u, vs, d, lane);
+  if (d <= 128) return sorted_sum_reg<4>(u, vs, d, lane);
+  if (d <= 256) return sorted_sum_reg<8>(u, vs, d, lane);
+  return sorted_sum_select(u, vs, d, lane);
+}
+
+// Finalize one instance's step (run by the whole block of its last variable tile).
+template <class T>
+__device__ void finalize_step(const PackView<T>& P, const InstDesc& I, int ii, double* red) {
+  double e = 0.0;
+  for (int i = threadIdx.x; i < I.nctile; i += kThreads) e = __dadd_rn(e, P.epart[I.ctile0 + i]);
+  e = block_sum_d(e, red);
+  if (threadIdx.x == 0) {
+    InstCtrl* S = P.ctrl + ii;
+    volatile InstCtrl* vS = S;
+    const int loc = vS->acc_loc;
+    const int vfail = vS->acc_vfail;
+    const int kmax = vS->acc_kmax;
+    S->loc = loc;
+    S->vfail = vfail;
+    S->energy = e;
+    if (loc < S->best_loc) {
+      S->best_loc = loc;
+      S->best_t = S->t;
+    }
+    const bool solved = (loc == 0 && vfail == 0);
+    if (solved) {
+      S->solved_step = S->step;
+      S->solved_t = S->t;
+      S->sol_set = S->set;
+      S->sol_k = S->kcur;
+    }
+    const int kacc = kmax < kTrials - 1 ? kmax : kTrials - 1;
+    const double hs = 0.125 / (double)(1 << kacc);
+    const double ht = kmax < kTrials ? hs : 0.0078125;
+    S->t = __dadd_rn(S->t, ht);
+    S->step += 1;
+    S->set ^= 1;
+    S->kcur = kacc;
+    S->h_state = hs;
+    S->pending = 1;
+    S->acc_loc = 0;
+    S->acc_vfail = 0;
+    S->acc_kmax = 0;
+    S->vtiles_done = 0;
+    int st = 0;
+    if (solved) st = 1;
+    else if (I.max_steps > 0 && S->step >= I.max_steps) st = 2;
+    if (st) {
+      S->done = st;
+      atomicSub(P.active, 1);
+      const int pos = atomicAdd(P.ring_tail, 1);
+      P.ring[pos % P.ring_cap] = ii;
+    }
+    __threadfence();
+  }
+}
+
+// Variable tiles.  MODE 0: integration step.  MODE 1: right-hand side only (writes dV).
+template <class T, int G, bool SORTED, int MODE>
+__global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restrict__ dv_out) {
+  __shared__ InstDesc s_inst;
+  __shared__ TileSnap s_snap;
+  __shared__ Tile s_tile;
+  __shared__ int s_ti, s_last;
+  __shared__ int s_km[kThreads / 32];
+  __shared__ double s_red[kThreads / 32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) P.queue[0] = 0;  // clause-tile queue is idle
+  const int ntiles = P.ntiles[1];
+  constexpr int VPP = kThreads / G;
+  const int grp = threadIdx.x / G, lane = threadIdx.x % G;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int ti = atomicAdd(&P.queue[1], 1);
+      s_ti = ti;
+      if (ti < ntiles) {
+        s_tile = P.vtiles[ti];
+        s_inst = P.inst[s_tile.inst];
+        const InstCtrl* S = P.ctrl + s_tile.inst;
+        s_snap.done = S->done;
+        s_snap.set = S->set;
+        s_snap.kcur = S->kcur;
+      }
+    }
+    __syncthreads();
+    const int ti = s_ti;
+    if (ti >= ntiles) break;
+    if (s_snap.done == 0) {
+      const InstDesc& I = s_inst;
+      const T* __restrict__ u = P.u + I.slot0;
+      const int32_t* __restrict__ vsl = P.vslot + I.slot0;
+      const int32_t* __restrict__ vend = P.vend + I.var0;
+      T* __restrict__ cur = P.cand + (int64_t)(s_snap.set * kTrials + s_snap.kcur) * P.var_cap + I.var0;
+      T* __restrict__ nxt = P.cand + (int64_t)((s_snap.set ^ 1) * kTrials) * P.var_cap + I.var0;
+      const int8_t* __restrict__ unit = P.unit + I.var0;
+      const int v_end = s_tile.begin + s_tile.count;
+      int kmax = 0;
+      for (int vb = s_tile.begin; vb < v_end; vb += VPP) {
+        const int v = vb + grp;
+        const bool valid = v < v_end;
+        int s0 = 0, s1 = 0;
+        if (valid) {
+          s1 = __ldg(vend + v);
+          s0 = v > 0 ? __ldg(vend + v - 1) : 0;
+        }
+        T dv;
+        if constexpr (SORTED) {
+          dv = T(sorted_sum(reinterpret_cast<const double*>(u), vsl + s0, s1 - s0, lane));
+        } else {
+          dv = tree_sum<T, G>(u, vsl + s0, s1 - s0, lane);
+        }
+        if (valid && lane == 0) {
+          if (MODE == 1) {
+            dv_out[v] = (double)dv;
+          } else {
+            const T V = cur[v];
+            const int8_t un = unit[v];
+            int kv = kTrials;
+#pragma unroll
+            for (int k = 0; k < kTrials; k++) {
+              const T h = T(0.125 / (double)(1 << k));
+              T c = add(V, mul(h, dv));
+              if (un != 0) c = T(un);
+              c = clampv(c, T(-1), T(1));
+              nxt[(int64_t)k * P.var_cap + v] = c;
+              const bool fail = fabs((double)c - (double)V) >= 1.0;
+              if (!fail && kv == kTrials) kv = k;
+            }
+            kmax = max(kmax, kv);
+          }
+        }
+      }
+      if (MODE == 0) {
+        kmax = warp_max_i(kmax);
+        if ((threadIdx.x & 31) == 0) s_km[threadIdx.x >> 5] = kmax;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          int km = 0;
+          for (int i = 0; i < kThreads / 32; i++) km = max(km, s_km[i]);
+          InstCtrl* S = P.ctrl + s_tile.inst;
+          if (km) atomicMax(&S->acc_kmax, km);
+          __threadfence();
+          const int prev = atomicAdd(&S->vtiles_done, 1);
+          s_last = (prev == I.nvtile - 1);
+        }
+        __syncthreads();
+        if (s_last) {
+          __threadfence();
+          finalize_step<T>(P, I, s_tile.inst, s_red);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- setup, state I/O and the reference function-pair mirrors ---------------------------
+
+// Occurrence count of every variable (the reference's numOccurrenceT, dynex.cc:2380-2383).
+__global__ void k_count(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ deg) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x)
+    atomicAdd(&deg[abs(lit[s]) - 1], 1);
+}
+
+// Inclusive scan, 2048 elements per block; block totals to `sums`.
+__global__ void k_scan_block(int32_t* __restrict__ a, int len, int32_t* __restrict__ sums) {
+  constexpr int IPT = 8;
+  __shared__ int32_t s[kThreads];
+  const int base = blockIdx.x * kThreads * IPT + threadIdx.x * IPT;
+  int32_t x[IPT];
+  int32_t run = 0;
+#pragma unroll
+  for (int i = 0; i < IPT; i++) {
+    x[i] = (base + i < len) ? a[base + i] : 0;
+    run += x[i];
+    x[i] = run;
+  }
+  s[threadIdx.x] = run;
+  __syncthreads();
+  for (int o = 1; o < kThreads; o <<= 1) {
+    const int32_t add_v = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += add_v;
+    __syncthreads();
+  }
+  const int32_t prefix = threadIdx.x > 0 ? s[threadIdx.x - 1] : 0;
+#pragma unroll
+  for (int i = 0; i < IPT; i++)
+    if (base + i < len) a[base + i] = x[i] + prefix;
+  if (threadIdx.x == kThreads - 1 && sums) sums[blockIdx.x] = s[kThreads - 1];
+}
+
+__global__ void k_scan_add(int32_t* __restrict__ a, int len, const int32_t* __restrict__ sums) {
+  constexpr int IPT = 8;
+  if (blockIdx.x == 0) return;
+  const int32_t add_v = sums[blockIdx.x - 1];
+  const int base = blockIdx.x * kThreads * IPT + threadIdx.x * IPT;
+#pragma unroll
+  for (int i = 0; i < IPT; i++)
+    if (base + i < len) a[base + i] += add_v;
+}
+
+__global__ void k_fill_start(const int32_t* __restrict__ vend, int n, int32_t* __restrict__ fill) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    fill[v] = v > 0 ? vend[v - 1] : 0;
+}
+
+__global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ fill,
+                          int32_t* __restrict__ vslot) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
+    const int pos = atomicAdd(&fill[abs(lit[s]) - 1], 1);
+    vslot[pos] = s;
+  }
+}
+
+// Sorts each variable's slot list ascending (warp per variable, bitonic in shared
+// memory) so the CSR is independent of the scatter's atomic order.  Lists longer than
+// kSortCap are reported in `longv` for the host.
+constexpr int kSortCap = 1024;
+__global__ void __launch_bounds__(kThreads) k_sort_lists(const int32_t* __restrict__ vend, int n,
+                                                         int32_t* __restrict__ vslot,
+                                                         int32_t* __restrict__ longv,
+                                                         int32_t* __restrict__ nlong) {
+  extern __shared__ int32_t sm[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int32_t* buf = sm + w * kSortCap;
+  for (int v = blockIdx.x * (kThreads / 32) + w; v < n; v += gridDim.x * (kThreads / 32)) {
+    const int s0 = v > 0 ? vend[v - 1] : 0, s1 = vend[v];
+    const int d = s1 - s0;
+    if (d <= 1) continue;
+    if (d > kSortCap) {
+      if (lane == 0) longv[atomicAdd(nlong, 1)] = v;
+      continue;
+    }
+    int N = 2;
+    while (N < d) N <<= 1;
+    for (int j = lane; j < N; j += 32) buf[j] = j < d ? vslot[s0 + j] : 0x7fffffff;
+    __syncwarp();
+    for (int k = 2; k <= N; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int e = lane; e < N; e += 32) {
+          const int p = e ^ j;
+          if (p > e) {
+            const bool up = (e & k) == 0;
+            const int32_t x = buf[e], y = buf[p];
+            if (up ? (y < x) : (x < y)) {
+              buf[e] = y;
+              buf[p] = x;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    for (int j = lane; j < d; j += 32) vslot[s0 + j] = buf[j];
+    __syncwarp();
+  }
+}
+
+// x (doubles, reference layout) -> V in cand[0][0], Xs, Xl.
+template <class T>
+__global__ void k_set_state(const double* __restrict__ x, int n, int m, T* __restrict__ V,
+                            T* __restrict__ Xs, T* __restrict__ Xl) {
+  const int64_t N = (int64_t)n + 2 * (int64_t)m;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const T v = T(x[i]);
+    if (i < n) V[i] = v;
+    else if (i < n + m) Xs[i - n] = v;
+    else Xl[i - n - m] = v;
+  }
+}
+
+// Current state (after the last accepted step) -> x doubles; applies a pending Xs/Xl
+// update without storing it.
+template <class T>
+__global__ void k_get_state(const InstDesc* __restrict__ insts, const InstCtrl* __restrict__ ctrl,
+                            int ii, const T* __restrict__ cand, int64_t var_cap,
+                            const T* __restrict__ Xs, const T* __restrict__ Xl,
+                            const T* __restrict__ Cp, const T* __restrict__ alpha_cm,
+                            double* __restrict__ x) {
+  const InstDesc I = insts[ii];
+  const InstCtrl S = ctrl[ii];
+  const ClauseConsts<T> kc = make_consts<T>(I, S.h_state);
+  const T* V = cand + (int64_t)(S.set * kTrials + S.kcur) * var_cap + I.var0;
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < I.n) {
+      x[i] = (double)V[i];
+    } else {
+      const int c = (int)((i < I.n + I.m) ? i - I.n : i - I.n - I.m);
+      T xs = Xs[I.cls0 + c], xl = Xl[I.cls0 + c];
+      if (S.pending) {
+        const T al = I.has_alpha_cm ? alpha_cm[I.cls0 + c] : kc.alpha;
+        advance_memory(xs, xl, Cp[I.cls0 + c], al, kc);
+      }
+      x[i] = (double)((i < I.n + I.m) ? xs : xl);
+    }
+  }
+}
+
+// dXs / dXl of every clause from the stored C_m (dynex.cc:503, 506), for the
+// right-hand-side mirror.  x/out: reference layout doubles.
+template <class T>
+__global__ void k_clause_dx(const InstDesc* __restrict__ insts, int ii, const T* __restrict__ Xs,
+                            const T* __restrict__ Cp, const T* __restrict__ alpha_cm,
+                            double* __restrict__ out) {
+  const InstDesc I = insts[ii];
+  const ClauseConsts<T> kc = make_consts<T>(I, 0.0);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < I.m; c += gridDim.x * blockDim.x) {
+    const T xs = clampv(Xs[I.cls0 + c], T(0), T(1));
+    const T C = Cp[I.cls0 + c];
+    const T al = I.has_alpha_cm ? alpha_cm[I.cls0 + c] : kc.alpha;
+    out[I.n + c] = (double)mul(mul(kc.beta, add(xs, kc.eps)), sub(C, kc.gamma));
+    out[I.n + I.m + c] = (double)mul(al, sub(C, kc.delta));
+  }
+}
+
+// One reference Euler step dmm_dostep (dynex.cc:301-327) on explicit vectors.
+template <class T>
+__global__ void k_dostep(const InstDesc* __restrict__ insts, int ii, const int8_t* __restrict__ unit,
+                         const double* __restrict__ x, const double* __restrict__ dx, double h,
+                         double* __restrict__ xo) {
+  const InstDesc I = insts[ii];
+  const T hh = T(h), one = T(1), xlmax = T(I.xl_max);
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T v = add(T(x[i]), mul(hh, T(dx[i])));
+    if (i < I.n) {
+      const int8_t un = unit[I.var0 + i];
+      if (un != 0) v = T(un);
+      v = clampv(v, -one, one);
+    } else if (i < I.n + I.m) {
+      v = clampv(v, T(0), one);
+    } else {
+      v = clampv(v, one, xlmax);
+    }
+    xo[i] = (double)v;
+  }
+}
+
+// Sum of an instance's energy partials and its loc/strict counters after a right-hand-side
+// evaluation; zeroes the accumulators.  One block.
+__global__ void k_rhs_finish(const InstDesc* __restrict__ insts, InstCtrl* __restrict__ ctrl, int ii,
+                             const double* __restrict__ epart) {
+  __shared__ double red[kThreads / 32];
+  const InstDesc I = insts[ii];
+  double e = 0.0;
+  for (int i = threadIdx.x; i < I.nctile; i += kThreads) e = __dadd_rn(e, epart[I.ctile0 + i]);
+  e = block_sum_d(e, red);
+  if (threadIdx.x == 0) {
+    InstCtrl* S = ctrl + ii;
+    S->energy = e;
+    S->loc = S->acc_loc;
+    S->vfail = S->acc_vfail;
+    S->acc_loc = 0;
+    S->acc_vfail = 0;
+    S->acc_kmax = 0;
+    S->vtiles_done = 0;
+  }
+}
+
+// Writes a large buffer so that the next kernel starts with a cold L2 (benchmarks).
+__global__ void k_flush(int4* __restrict__ buf, int64_t n16, int salt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16;
+       i += (int64_t)gridDim.x * blockDim.x)
+    buf[i] = make_int4(salt, (int)i, salt, (int)i);
+}
+
+}  // namespace dmm

@@ -1,0 +1,1010 @@
+// Pack: device arrays, device-built CSR, tile tables and the CUDA-graph step loop.
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "dmm_kernels.cuh"
+#include "dmm_pack.h"
+
+namespace dmm {
+
+// ---- errors --------------------------------------------------------------------------------
+static thread_local std::string g_err;
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+void clear_error() { g_err.clear(); }
+const char* last_error() { return g_err.c_str(); }
+
+dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
+                            bool* k3) {
+  if (n <= 0 || m < 0 || clause_off == nullptr) {
+    set_error("formula: need n > 0, m >= 0 and clause offsets");
+    return DMM_ERR_ARG;
+  }
+  if (clause_off[0] != 0) {
+    set_error("formula: clause_off[0] must be 0");
+    return DMM_ERR_ARG;
+  }
+  bool all3 = m > 0;
+  for (int32_t c = 0; c < m; c++) {
+    const int64_t len = clause_off[c + 1] - clause_off[c];
+    if (len < 0) {
+      set_error("formula: clause offsets decrease at clause %d", c);
+      return DMM_ERR_ARG;
+    }
+    if (len > DMM_MAX_CLAUSE_LITS) {
+      set_error("CLAUSE %d HAS MORE THAN %d LITERALS", c, DMM_MAX_CLAUSE_LITS);
+      return DMM_ERR_CLAUSE_LEN;
+    }
+    if (len != 3) all3 = false;
+  }
+  const int64_t L = clause_off[m];
+  if (L > 0x7fffffffll - 64) {
+    set_error("formula: %lld literals exceed the 2^31 slot limit", (long long)L);
+    return DMM_ERR_ARG;
+  }
+  if (L > 0 && lits == nullptr) {
+    set_error("formula: literals missing");
+    return DMM_ERR_ARG;
+  }
+  for (int64_t s = 0; s < L; s++) {
+    const int32_t l = lits[s];
+    if (l == 0 || l > n || l < -n) {
+      set_error("formula: literal %d at position %lld out of range for n=%d", l, (long long)s, n);
+      return DMM_ERR_LITERAL;
+    }
+  }
+  *k3 = all3;
+  return DMM_OK;
+}
+
+// ---- range allocator ---------------------------------------------------------------------------
+void RangeAlloc::reset(int64_t cap) {
+  free_.clear();
+  if (cap > 0) free_[0] = cap;
+}
+
+int64_t RangeAlloc::alloc(int64_t len) {
+  len = round(std::max<int64_t>(len, 1));
+  for (auto it = free_.begin(); it != free_.end(); ++it) {
+    if (it->second >= len) {
+      const int64_t start = it->first, rest = it->second - len;
+      free_.erase(it);
+      if (rest > 0) free_[start + len] = rest;
+      return start;
+    }
+  }
+  return -1;
+}
+
+void RangeAlloc::free(int64_t start, int64_t len) {
+  len = round(std::max<int64_t>(len, 1));
+  auto it = free_.emplace(start, len).first;
+  auto nx = std::next(it);
+  if (nx != free_.end() && it->first + it->second == nx->first) {
+    it->second += nx->second;
+    free_.erase(nx);
+  }
+  if (it != free_.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) {
+      pv->second += it->second;
+      free_.erase(it);
+    }
+  }
+}
+
+int64_t RangeAlloc::largest_free() const {
+  int64_t b = 0;
+  for (auto& kv : free_) b = std::max(b, kv.second);
+  return b;
+}
+
+// ---- pack ------------------------------------------------------------------------------------
+
+namespace {
+inline int blocks_for(int64_t work, int per = kThreads, int cap = 148 * 16) {
+  int64_t b = (work + per - 1) / per;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+constexpr int kClauseTileUnit = 4 * kThreads;  // clauses per pass of the vector path
+constexpr int kVarTileUnit = kThreads;          // variables per tile unit
+}  // namespace
+
+int64_t Pack::bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
+                        bool with_alpha_cm) {
+  const int64_t t = prec == DMM_FP64 ? 8 : 4;
+  n = RangeAlloc::round(std::max<int64_t>(n, 1));
+  m = RangeAlloc::round(std::max<int64_t>(m, 1));
+  slots = RangeAlloc::round(std::max<int64_t>(slots, 1));
+  int64_t b = m * (3 * t + 4 + (with_alpha_cm ? t : 0)) + slots * (8 + t) + n * (8 * t + 9);
+  b += (m / kClauseTileUnit + 1) * (8 + 16) + (n / kVarTileUnit + 1) * 16;
+  b += sizeof(InstDesc) + sizeof(InstCtrl) + 8;
+  return b;
+}
+
+Pack::~Pack() {
+  if (dev_ >= 0) cudaSetDevice(dev_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  void* ptrs[] = {Xs_,      Xl_,        Cp_,      alpha_cm_,   u_,         cand_,
+                  coff_,    lit_,       vslot_,   vend_,       fill_,      unit_,
+                  epart_,   inst_d_,    ctrl_d_,  ctiles_d_,   vtiles_d_,  ntiles_d_,
+                  queue_d_, active_d_,  ring_d_,  ring_tail_d_, scan_tmp_, longv_d_,
+                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (pinned_) cudaFreeHost(pinned_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_grid) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return DMM_ERR_NO_DEVICE;
+  }
+  if (dev_ < 0 || dev_ >= ndev) {
+    set_error("device %d out of range (%d devices)", dev_, ndev);
+    return DMM_ERR_ARG;
+  }
+  DMM_CUDA(cudaSetDevice(dev_));
+  DMM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  DMM_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev_));
+  for (auto& e : ev_) DMM_CUDA(cudaEventCreate(&e));
+  with_alpha_cm_ = with_alpha_cm;
+  fixed_grid_ = fixed_grid;
+  tsize_ = prec_ == DMM_FP64 ? 8 : 4;
+  caps_ = caps_in;
+  if (caps_.insts < 1) caps_.insts = 1;
+  caps_.vars = RangeAlloc::round(caps_.vars) + 32 * (int64_t)caps_.insts;
+  caps_.clauses = RangeAlloc::round(caps_.clauses) + 32 * (int64_t)caps_.insts;
+  caps_.slots = RangeAlloc::round(caps_.slots) + 32 * (int64_t)caps_.insts;
+  const int64_t V = caps_.vars, C = caps_.clauses, S = caps_.slots, I = caps_.insts;
+  ctile_cap_ = C / kClauseTileUnit + I + 1;
+  vtile_cap_ = V / kVarTileUnit + I + 1;
+  DMM_CUDA(cudaMalloc(&Xs_, C * tsize_));
+  DMM_CUDA(cudaMalloc(&Xl_, C * tsize_));
+  DMM_CUDA(cudaMalloc(&Cp_, C * tsize_));
+  if (with_alpha_cm) DMM_CUDA(cudaMalloc(&alpha_cm_, C * tsize_));
+  DMM_CUDA(cudaMalloc(&coff_, C * 4));
+  DMM_CUDA(cudaMalloc(&lit_, S * 4));
+  DMM_CUDA(cudaMalloc(&vslot_, S * 4));
+  DMM_CUDA(cudaMalloc(&u_, S * tsize_));
+  DMM_CUDA(cudaMalloc(&cand_, 2 * kTrials * V * tsize_));
+  DMM_CUDA(cudaMalloc(&vend_, V * 4));
+  DMM_CUDA(cudaMalloc(&fill_, V * 4));
+  DMM_CUDA(cudaMalloc(&unit_, V));
+  DMM_CUDA(cudaMalloc(&epart_, ctile_cap_ * sizeof(double)));
+  DMM_CUDA(cudaMalloc(&inst_d_, I * sizeof(InstDesc)));
+  DMM_CUDA(cudaMalloc(&ctrl_d_, I * sizeof(InstCtrl)));
+  DMM_CUDA(cudaMalloc(&ctiles_d_, ctile_cap_ * sizeof(Tile)));
+  DMM_CUDA(cudaMalloc(&vtiles_d_, vtile_cap_ * sizeof(Tile)));
+  DMM_CUDA(cudaMalloc(&ntiles_d_, 4 * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&queue_d_, 2 * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&active_d_, sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&ring_d_, I * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&ring_tail_d_, 4 * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
+  DMM_CUDA(cudaMemsetAsync(ctrl_d_, 0, I * sizeof(InstCtrl), stream_));
+  DMM_CUDA(cudaMemsetAsync(ntiles_d_, 0, 4 * sizeof(int32_t), stream_));
+  DMM_CUDA(cudaMemsetAsync(queue_d_, 0, 2 * sizeof(int32_t), stream_));
+  DMM_CUDA(cudaMemsetAsync(active_d_, 0, sizeof(int32_t), stream_));
+  DMM_CUDA(cudaMemsetAsync(ring_tail_d_, 0, 4 * sizeof(int32_t), stream_));
+  DMM_CUDA(cudaMemsetAsync(cand_, 0, 2 * kTrials * V * tsize_, stream_));
+  var_alloc_.reset(V);
+  cls_alloc_.reset(C);
+  slot_alloc_.reset(S);
+  inst_h_.assign(I, InstDesc{});
+  live_.assign(I, 0);
+  tun_ = dmm_tuning{};
+  DMM_TRY(set_tuning(&tun_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::set_tuning(const dmm_tuning* t) {
+  dmm_tuning n = *t;
+  if (n.clause_tile <= 0) n.clause_tile = kClauseTileUnit;
+  if (n.clause_tile % kClauseTileUnit) {
+    set_error("clause_tile must be a multiple of %d", kClauseTileUnit);
+    return DMM_ERR_ARG;
+  }
+  if (prec_ == DMM_FP64) {
+    if (n.var_group != 0 && n.var_group != 32) {
+      set_error("FP64 mode reduces with one warp per variable (var_group 32)");
+      return DMM_ERR_ARG;
+    }
+    n.var_group = 32;
+  } else {
+    if (n.var_group <= 0) n.var_group = 8;
+    if (n.var_group != 1 && n.var_group != 2 && n.var_group != 4 && n.var_group != 8 &&
+        n.var_group != 16 && n.var_group != 32) {
+      set_error("var_group must be 1, 2, 4, 8, 16 or 32");
+      return DMM_ERR_ARG;
+    }
+  }
+  if (n.var_tile <= 0) n.var_tile = kVarTileUnit;
+  if (n.var_tile % kVarTileUnit) {
+    set_error("var_tile must be a multiple of %d", kVarTileUnit);
+    return DMM_ERR_ARG;
+  }
+  if (n.steps_per_graph <= 0) n.steps_per_graph = 32;
+  if (n.steps_per_graph > 4096) n.steps_per_graph = 4096;
+  if (n.blocks_per_sm < 0 || n.blocks_per_sm > 32) {
+    set_error("blocks_per_sm out of range");
+    return DMM_ERR_ARG;
+  }
+  const bool retile = n.clause_tile != tun_.clause_tile || n.var_tile != tun_.var_tile;
+  tun_ = n;
+  graph_stale_ = true;
+  if (retile && !ctiles_h_.empty()) return commit_tiles();
+  if (!ctiles_h_.empty() || !vtiles_h_.empty()) return commit_tiles();
+  return DMM_OK;
+}
+
+int32_t Pack::num_live() const {
+  int32_t c = 0;
+  for (auto l : live_) c += l;
+  return c;
+}
+
+int32_t Pack::free_insts() const {
+  int32_t c = 0;
+  for (auto l : live_) c += !l;
+  return c;
+}
+
+dmm_status Pack::ensure_stage(int64_t doubles) {
+  if (doubles <= stage_cap_) return DMM_OK;
+  if (stage_) DMM_CUDA(cudaFree(stage_));
+  stage_ = nullptr;
+  stage_cap_ = 0;
+  DMM_CUDA(cudaMalloc(&stage_, doubles * sizeof(double)));
+  stage_cap_ = doubles;
+  return DMM_OK;
+}
+
+dmm_status Pack::upload_desc(int32_t idx) {
+  DMM_CUDA(cudaMemcpyAsync(inst_d_ + idx, &inst_h_[idx], sizeof(InstDesc), cudaMemcpyHostToDevice,
+                           stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::write_ctrl(int32_t idx, const InstCtrl& c) {
+  DMM_CUDA(cudaMemcpyAsync(ctrl_d_ + idx, &c, sizeof(InstCtrl), cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+__global__ void k_active_add(int32_t* a, int32_t d) { atomicAdd(a, d); }
+
+dmm_status Pack::add_active(int32_t delta) {
+  k_active_add<<<1, 1, 0, stream_>>>(active_d_, delta);
+  DMM_CUDA(cudaGetLastError());
+  return DMM_OK;
+}
+
+dmm_status Pack::read_ctrl(int32_t idx, InstCtrl* c) {
+  if (!live(idx)) {
+    set_error("instance %d is not live", idx);
+    return DMM_ERR_ARG;
+  }
+  DMM_CUDA(cudaMemcpyAsync(c, ctrl_d_ + idx, sizeof(InstCtrl), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::read_ctrls(std::vector<InstCtrl>* out) {
+  out->resize(caps_.insts);
+  DMM_CUDA(cudaMemcpyAsync(out->data(), ctrl_d_, caps_.insts * sizeof(InstCtrl),
+                           cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+static dmm_status scan_inclusive(int32_t* a, int64_t len, int32_t* tmp, cudaStream_t s) {
+  constexpr int per = kThreads * 8;
+  const int64_t nb = (len + per - 1) / per;
+  if (nb <= 1) {
+    k_scan_block<<<1, kThreads, 0, s>>>(a, (int)len, nullptr);
+    DMM_CUDA(cudaGetLastError());
+    return DMM_OK;
+  }
+  k_scan_block<<<(unsigned)nb, kThreads, 0, s>>>(a, (int)len, tmp);
+  DMM_CUDA(cudaGetLastError());
+  DMM_TRY(scan_inclusive(tmp, nb, tmp + nb, s));
+  k_scan_add<<<(unsigned)nb, kThreads, 0, s>>>(a, (int)len, tmp);
+  DMM_CUDA(cudaGetLastError());
+  return DMM_OK;
+}
+
+dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
+  const int n = I.n, L = I.nslots;
+  int32_t* vend = vend_ + I.var0;
+  int32_t* fill = fill_ + I.var0;
+  const int32_t* lit = lit_ + I.slot0;
+  int32_t* vsl = vslot_ + I.slot0;
+  DMM_CUDA(cudaMemsetAsync(vend, 0, (size_t)n * 4, stream_));
+  if (L > 0) {
+    k_count<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, vend);
+    DMM_CUDA(cudaGetLastError());
+  }
+  const int64_t need = n / (kThreads * 8) + 64;
+  if (need > scan_tmp_cap_) {
+    if (scan_tmp_) DMM_CUDA(cudaFree(scan_tmp_));
+    scan_tmp_ = nullptr;
+    DMM_CUDA(cudaMalloc(&scan_tmp_, need * 2 * sizeof(int32_t)));
+    scan_tmp_cap_ = need;
+  }
+  DMM_TRY(scan_inclusive(vend, n, scan_tmp_, stream_));
+  k_fill_start<<<blocks_for(n), kThreads, 0, stream_>>>(vend, n, fill);
+  DMM_CUDA(cudaGetLastError());
+  if (L > 0) {
+    k_scatter<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, fill, vsl);
+    DMM_CUDA(cudaGetLastError());
+  }
+  int32_t* nlong = ring_tail_d_ + 2;
+  DMM_CUDA(cudaMemsetAsync(nlong, 0, sizeof(int32_t), stream_));
+  const size_t smem = (kThreads / 32) * kSortCap * sizeof(int32_t);
+  k_sort_lists<<<blocks_for(n, kThreads / 32), kThreads, smem, stream_>>>(vend, n, vsl, longv_d_,
+                                                                          nlong);
+  DMM_CUDA(cudaGetLastError());
+  int32_t h_nlong = 0;
+  DMM_CUDA(cudaMemcpyAsync(&h_nlong, nlong, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  if (h_nlong > 0) {
+    // Lists longer than the shared-memory sorter: sorted on the host (setup only).
+    std::vector<int32_t> ids(h_nlong), ends(n);
+    DMM_CUDA(cudaMemcpy(ids.data(), longv_d_, h_nlong * 4, cudaMemcpyDeviceToHost));
+    DMM_CUDA(cudaMemcpy(ends.data(), vend, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    std::vector<int32_t> seg;
+    for (int32_t v : ids) {
+      const int s0 = v > 0 ? ends[v - 1] : 0, s1 = ends[v];
+      seg.resize(s1 - s0);
+      DMM_CUDA(cudaMemcpy(seg.data(), vsl + s0, seg.size() * 4, cudaMemcpyDeviceToHost));
+      std::sort(seg.begin(), seg.end());
+      DMM_CUDA(cudaMemcpy(vsl + s0, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  (void)lits_host;
+  return DMM_OK;
+}
+
+static double effective_xl_max(int32_t factor, int32_t m) {
+  int32_t v = (int32_t)((uint32_t)factor * (uint32_t)m);  // dynex.cc:2358 in int arithmetic
+  if (v <= 0) v = 0x7fffffff;
+  return (double)v;
+}
+
+static void fill_params(InstDesc& I, const dmm_params* p) {
+  dmm_params d;
+  dmm_params_default(&d);
+  if (!p) p = &d;
+  I.alpha = p->alpha;
+  I.beta = p->beta;
+  I.gamma = p->gamma;
+  I.delta = p->delta;
+  I.eps = p->epsilon;
+  I.zeta = p->zeta;
+  I.xl_max = effective_xl_max(p->xl_max, I.m);
+}
+
+template <class T>
+static dmm_status upload_alpha(T* dst, const double* a, int32_t m, cudaStream_t s) {
+  std::vector<T> h(m);
+  for (int32_t i = 0; i < m; i++) h[i] = T(a[i]);
+  DMM_CUDA(cudaMemcpyAsync(dst, h.data(), (size_t)m * sizeof(T), cudaMemcpyHostToDevice, s));
+  DMM_CUDA(cudaStreamSynchronize(s));
+  return DMM_OK;
+}
+
+dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
+                     const dmm_params* p, const double* alpha_cm, int32_t max_steps,
+                     int32_t* idx_out) {
+  bool k3 = false;
+  DMM_TRY(validate_formula(lits, clause_off, n, m, &k3));
+  if (alpha_cm && !with_alpha_cm_) {
+    set_error("this pack was created without per-clause alpha storage");
+    return DMM_ERR_ARG;
+  }
+  DMM_CUDA(cudaSetDevice(dev_));
+  int32_t idx = -1;
+  for (int32_t i = 0; i < (int32_t)live_.size(); i++)
+    if (!live_[i]) {
+      idx = i;
+      break;
+    }
+  if (idx < 0) {
+    set_error("pack is full (%d instances)", caps_.insts);
+    return DMM_ERR_BUDGET;
+  }
+  const int64_t L = clause_off[m];
+  const int64_t var0 = var_alloc_.alloc(n);
+  const int64_t cls0 = var0 < 0 ? -1 : cls_alloc_.alloc(m);
+  const int64_t slot0 = cls0 < 0 ? -1 : slot_alloc_.alloc(L);
+  if (var0 < 0 || cls0 < 0 || slot0 < 0) {
+    if (var0 >= 0) var_alloc_.free(var0, n);
+    if (cls0 >= 0) cls_alloc_.free(cls0, m);
+    set_error("pack capacity exhausted (n=%d m=%d literals=%lld)", n, m, (long long)L);
+    return DMM_ERR_BUDGET;
+  }
+  InstDesc I{};
+  I.n = n;
+  I.m = m;
+  I.var0 = var0;
+  I.cls0 = cls0;
+  I.slot0 = slot0;
+  I.nslots = (int32_t)L;
+  I.k3 = k3 ? 1 : 0;
+  I.has_alpha_cm = alpha_cm ? 1 : 0;
+  I.max_steps = max_steps;
+  fill_params(I, p);
+  if (L > 0)
+    DMM_CUDA(cudaMemcpyAsync(lit_ + slot0, lits, (size_t)L * 4, cudaMemcpyHostToDevice, stream_));
+  std::vector<int32_t> coff_local;
+  if (!k3 && m > 0) {
+    coff_local.resize(m);
+    for (int32_t c = 0; c < m; c++) coff_local[c] = (int32_t)clause_off[c];
+    DMM_CUDA(cudaMemcpyAsync(coff_ + cls0, coff_local.data(), (size_t)m * 4,
+                             cudaMemcpyHostToDevice, stream_));
+  }
+  // unit clauses (dynex.cc:2459-2469: the last unit clause of a variable wins)
+  std::vector<int8_t> unit(n, 0);
+  for (int32_t c = 0; c < m; c++)
+    if (clause_off[c + 1] - clause_off[c] == 1) {
+      const int32_t l = lits[clause_off[c]];
+      unit[std::abs(l) - 1] = l > 0 ? 1 : -1;
+    }
+  DMM_CUDA(cudaMemcpyAsync(unit_ + var0, unit.data(), n, cudaMemcpyHostToDevice, stream_));
+  if (alpha_cm) {
+    if (prec_ == DMM_FP64)
+      DMM_TRY(upload_alpha(static_cast<double*>(alpha_cm_) + cls0, alpha_cm, m, stream_));
+    else
+      DMM_TRY(upload_alpha(static_cast<float*>(alpha_cm_) + cls0, alpha_cm, m, stream_));
+  }
+  DMM_TRY(build_csr(I, lits));
+  inst_h_[idx] = I;
+  live_[idx] = 1;
+  DMM_TRY(upload_desc(idx));
+  InstCtrl c{};
+  c.done = DMM_CANCELLED;  // not runnable until a state is set
+  c.best_loc = m;
+  c.loc = m;
+  c.solved_step = -1;
+  c.solved_t = -1.0;
+  c.h_state = 0.125;
+  DMM_TRY(write_ctrl(idx, c));
+  if (!fixed_grid_) graph_stale_ = true;
+  *idx_out = idx;
+  return DMM_OK;
+}
+
+dmm_status Pack::remove(int32_t idx) {
+  if (!live(idx)) {
+    set_error("instance %d is not live", idx);
+    return DMM_ERR_ARG;
+  }
+  InstCtrl c;
+  DMM_TRY(read_ctrl(idx, &c));
+  if (c.done == 0) {
+    DMM_TRY(add_active(-1));
+    c.done = DMM_CANCELLED;
+    DMM_TRY(write_ctrl(idx, c));
+  }
+  const InstDesc& I = inst_h_[idx];
+  var_alloc_.free(I.var0, I.n);
+  cls_alloc_.free(I.cls0, I.m);
+  slot_alloc_.free(I.slot0, I.nslots);
+  live_[idx] = 0;
+  if (!fixed_grid_) graph_stale_ = true;
+  return DMM_OK;
+}
+
+dmm_status Pack::set_params(int32_t idx, const dmm_params* p, const double* alpha_cm) {
+  if (!live(idx)) return DMM_ERR_ARG;
+  if (alpha_cm && !with_alpha_cm_) {
+    set_error("this pack was created without per-clause alpha storage");
+    return DMM_ERR_ARG;
+  }
+  InstDesc& I = inst_h_[idx];
+  fill_params(I, p);
+  I.has_alpha_cm = alpha_cm ? 1 : 0;
+  if (alpha_cm) {
+    if (prec_ == DMM_FP64)
+      DMM_TRY(upload_alpha(static_cast<double*>(alpha_cm_) + I.cls0, alpha_cm, I.m, stream_));
+    else
+      DMM_TRY(upload_alpha(static_cast<float*>(alpha_cm_) + I.cls0, alpha_cm, I.m, stream_));
+  }
+  DMM_TRY(upload_desc(idx));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::set_max_steps(int32_t idx, int32_t max_steps) {
+  if (!live(idx)) return DMM_ERR_ARG;
+  inst_h_[idx].max_steps = max_steps;
+  DMM_TRY(upload_desc(idx));
+  return DMM_OK;
+}
+
+dmm_status Pack::set_state(int32_t idx, const double* x) {
+  if (!live(idx) || !x) {
+    set_error("set_state: bad instance or null state");
+    return DMM_ERR_ARG;
+  }
+  const InstDesc& I = inst_h_[idx];
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  DMM_TRY(ensure_stage(3 * N));
+  InstCtrl old;
+  DMM_TRY(read_ctrl(idx, &old));
+  DMM_CUDA(cudaMemcpyAsync(stage_, x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  if (prec_ == DMM_FP64) {
+    double* V = static_cast<double*>(cand_) + I.var0;
+    k_set_state<double><<<blocks_for(N), kThreads, 0, stream_>>>(
+        stage_, I.n, I.m, V, static_cast<double*>(Xs_) + I.cls0, static_cast<double*>(Xl_) + I.cls0);
+  } else {
+    float* V = static_cast<float*>(cand_) + I.var0;
+    k_set_state<float><<<blocks_for(N), kThreads, 0, stream_>>>(
+        stage_, I.n, I.m, V, static_cast<float*>(Xs_) + I.cls0, static_cast<float*>(Xl_) + I.cls0);
+  }
+  DMM_CUDA(cudaGetLastError());
+  InstCtrl c{};
+  c.done = 0;
+  c.loc = I.m;
+  c.best_loc = I.m;
+  c.solved_step = -1;
+  c.solved_t = -1.0;
+  c.h_state = 0.125;
+  if (old.done != 0) DMM_TRY(add_active(+1));
+  DMM_TRY(write_ctrl(idx, c));
+  return DMM_OK;
+}
+
+dmm_status Pack::get_state(int32_t idx, double* x, double* t) {
+  if (!live(idx)) return DMM_ERR_ARG;
+  const InstDesc& I = inst_h_[idx];
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  DMM_TRY(ensure_stage(3 * N));
+  if (prec_ == DMM_FP64) {
+    k_get_state<double><<<blocks_for(N), kThreads, 0, stream_>>>(
+        inst_d_, ctrl_d_, idx, static_cast<double*>(cand_), caps_.vars, static_cast<double*>(Xs_),
+        static_cast<double*>(Xl_), static_cast<double*>(Cp_), static_cast<double*>(alpha_cm_), stage_);
+  } else {
+    k_get_state<float><<<blocks_for(N), kThreads, 0, stream_>>>(
+        inst_d_, ctrl_d_, idx, static_cast<float*>(cand_), caps_.vars, static_cast<float*>(Xs_),
+        static_cast<float*>(Xl_), static_cast<float*>(Cp_), static_cast<float*>(alpha_cm_), stage_);
+  }
+  DMM_CUDA(cudaGetLastError());
+  if (x) DMM_CUDA(cudaMemcpyAsync(x, stage_, N * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  if (t) {
+    InstCtrl c;
+    DMM_TRY(read_ctrl(idx, &c));
+    *t = c.t;
+  }
+  return DMM_OK;
+}
+
+template <class T>
+void Pack::fill_view(void* vv) const {
+  PackView<T>& v = *static_cast<PackView<T>*>(vv);
+  v.Xs = static_cast<T*>(Xs_);
+  v.Xl = static_cast<T*>(Xl_);
+  v.Cp = static_cast<T*>(Cp_);
+  v.alpha_cm = static_cast<const T*>(alpha_cm_);
+  v.coff = coff_;
+  v.lit = lit_;
+  v.u = static_cast<T*>(u_);
+  v.vslot = vslot_;
+  v.vend = vend_;
+  v.cand = static_cast<T*>(cand_);
+  v.var_cap = caps_.vars;
+  v.unit = unit_;
+  v.epart = epart_;
+  v.inst = inst_d_;
+  v.ctrl = ctrl_d_;
+  v.ctiles = use_aux_ ? aux_ctiles_d_ : ctiles_d_;
+  v.vtiles = use_aux_ ? aux_vtiles_d_ : vtiles_d_;
+  v.ntiles = use_aux_ ? ntiles_d_ + 2 : ntiles_d_;
+  v.queue = queue_d_;
+  v.active = active_d_;
+  v.ring = ring_d_;
+  v.ring_tail = ring_tail_d_;
+  v.ring_cap = caps_.insts;
+}
+
+dmm_status Pack::enqueue_clause() {
+  if (prec_ == DMM_FP64) {
+    PackView<double> v;
+    fill_view<double>(&v);
+    k_clause<double, false><<<grid_c_, kThreads, 0, stream_>>>(v);
+  } else {
+    PackView<float> v;
+    fill_view<float>(&v);
+    k_clause<float, true><<<grid_c_, kThreads, 0, stream_>>>(v);
+  }
+  DMM_CUDA(cudaGetLastError());
+  return DMM_OK;
+}
+
+template <int MODE>
+static void launch_var_f32(int G, int grid, cudaStream_t s, const PackView<float>& v, double* dv) {
+  switch (G) {
+    case 1: k_var<float, 1, false, MODE><<<grid, kThreads, 0, s>>>(v, dv); break;
+    case 2: k_var<float, 2, false, MODE><<<grid, kThreads, 0, s>>>(v, dv); break;
+    case 4: k_var<float, 4, false, MODE><<<grid, kThreads, 0, s>>>(v, dv); break;
+    case 8: k_var<float, 8, false, MODE><<<grid, kThreads, 0, s>>>(v, dv); break;
+    case 16: k_var<float, 16, false, MODE><<<grid, kThreads, 0, s>>>(v, dv); break;
+    default: k_var<float, 32, false, MODE><<<grid, kThreads, 0, s>>>(v, dv); break;
+  }
+}
+
+dmm_status Pack::enqueue_var(bool rhs_only, void* dv_out) {
+  double* dv = static_cast<double*>(dv_out);
+  if (prec_ == DMM_FP64) {
+    PackView<double> v;
+    fill_view<double>(&v);
+    if (rhs_only)
+      k_var<double, 32, true, 1><<<grid_v_, kThreads, 0, stream_>>>(v, dv);
+    else
+      k_var<double, 32, true, 0><<<grid_v_, kThreads, 0, stream_>>>(v, dv);
+  } else {
+    PackView<float> v;
+    fill_view<float>(&v);
+    if (rhs_only)
+      launch_var_f32<1>(tun_.var_group, grid_v_, stream_, v, dv);
+    else
+      launch_var_f32<0>(tun_.var_group, grid_v_, stream_, v, dv);
+  }
+  DMM_CUDA(cudaGetLastError());
+  return DMM_OK;
+}
+
+dmm_status Pack::enqueue_step(bool rhs_only, void* dv_out) {
+  DMM_TRY(enqueue_clause());
+  DMM_TRY(enqueue_var(rhs_only, dv_out));
+  return DMM_OK;
+}
+
+static int occupancy_blocks(const void* fn) {
+  int b = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    b = 4;
+  }
+  return std::max(1, b);
+}
+
+dmm_status Pack::commit_tiles() {
+  ctiles_h_.clear();
+  vtiles_h_.clear();
+  const int TC = tun_.clause_tile, TV = tun_.var_tile;
+  for (int32_t i = 0; i < (int32_t)live_.size(); i++) {
+    if (!live_[i]) continue;
+    InstDesc& I = inst_h_[i];
+    I.ctile0 = (int32_t)ctiles_h_.size();
+    for (int32_t b = 0; b < I.m; b += TC) ctiles_h_.push_back(Tile{i, b, std::min(TC, I.m - b), 0});
+    I.nctile = (int32_t)ctiles_h_.size() - I.ctile0;
+    I.vtile0 = (int32_t)vtiles_h_.size();
+    for (int32_t b = 0; b < I.n; b += TV) vtiles_h_.push_back(Tile{i, b, std::min(TV, I.n - b), 0});
+    I.nvtile = (int32_t)vtiles_h_.size() - I.vtile0;
+    DMM_TRY(upload_desc(i));
+  }
+  if ((int64_t)ctiles_h_.size() > ctile_cap_ || (int64_t)vtiles_h_.size() > vtile_cap_) {
+    set_error("tile tables overflow");
+    return DMM_ERR_BUDGET;
+  }
+  if (!ctiles_h_.empty())
+    DMM_CUDA(cudaMemcpyAsync(ctiles_d_, ctiles_h_.data(), ctiles_h_.size() * sizeof(Tile),
+                             cudaMemcpyHostToDevice, stream_));
+  if (!vtiles_h_.empty())
+    DMM_CUDA(cudaMemcpyAsync(vtiles_d_, vtiles_h_.data(), vtiles_h_.size() * sizeof(Tile),
+                             cudaMemcpyHostToDevice, stream_));
+  int32_t nt[2] = {(int32_t)ctiles_h_.size(), (int32_t)vtiles_h_.size()};
+  DMM_CUDA(cudaMemcpyAsync(ntiles_d_, nt, sizeof nt, cudaMemcpyHostToDevice, stream_));
+  int bc, bv;
+  if (prec_ == DMM_FP64) {
+    bc = occupancy_blocks((const void*)k_clause<double, false>);
+    bv = occupancy_blocks((const void*)k_var<double, 32, true, 0>);
+  } else {
+    bc = occupancy_blocks((const void*)k_clause<float, true>);
+    bv = occupancy_blocks((const void*)k_var<float, 8, false, 0>);
+  }
+  if (tun_.blocks_per_sm > 0) {
+    bc = std::min(bc, tun_.blocks_per_sm);
+    bv = std::min(bv, tun_.blocks_per_sm);
+  }
+  const int gc = bc * sms_, gv = bv * sms_;
+  const int new_c = fixed_grid_ ? gc : std::max(1, std::min<int>(gc, nt[0]));
+  const int new_v = fixed_grid_ ? gv : std::max(1, std::min<int>(gv, nt[1]));
+  if (new_c != grid_c_ || new_v != grid_v_) graph_stale_ = true;
+  grid_c_ = new_c;
+  grid_v_ = new_v;
+  if (!fixed_grid_) graph_stale_ = true;
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::capture(int32_t steps) {
+  if (graph_exec_) {
+    DMM_CUDA(cudaGraphExecDestroy(graph_exec_));
+    graph_exec_ = nullptr;
+  }
+  if (graph_) {
+    DMM_CUDA(cudaGraphDestroy(graph_));
+    graph_ = nullptr;
+  }
+  DMM_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  dmm_status st = DMM_OK;
+  for (int32_t s = 0; s < steps && st == DMM_OK; s++) st = enqueue_step(false, nullptr);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(stream_, &g);
+  if (st != DMM_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  DMM_CUDA(e);
+  graph_ = g;
+  DMM_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+  graph_steps_ = steps;
+  graph_stale_ = false;
+  return DMM_OK;
+}
+
+dmm_status Pack::launch_steps(int32_t nsteps) {
+  DMM_CUDA(cudaSetDevice(dev_));
+  if (ctiles_h_.empty() && vtiles_h_.empty()) return DMM_OK;
+  const int32_t S = tun_.steps_per_graph;
+  while (nsteps >= S) {
+    if (graph_stale_ || graph_steps_ != S || !graph_exec_) DMM_TRY(capture(S));
+    DMM_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+    nsteps -= S;
+  }
+  for (int32_t s = 0; s < nsteps; s++) DMM_TRY(enqueue_step(false, nullptr));
+  return DMM_OK;
+}
+
+dmm_status Pack::profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t) {
+  DMM_CUDA(cudaSetDevice(dev_));
+  if (flush_bytes > flush_cap_) {
+    if (flush_) DMM_CUDA(cudaFree(flush_));
+    flush_ = nullptr;
+    DMM_CUDA(cudaMalloc(&flush_, flush_bytes));
+    flush_cap_ = flush_bytes;
+  }
+  for (int32_t s = 0; s < nsteps; s++) {
+    if (flush_bytes > 0) {
+      k_flush<<<sms_ * 4, kThreads, 0, stream_>>>(static_cast<int4*>(flush_), flush_bytes / 16, s);
+      DMM_CUDA(cudaGetLastError());
+    }
+    DMM_CUDA(cudaEventRecord(ev_[0], stream_));
+    DMM_TRY(enqueue_clause());
+    DMM_CUDA(cudaEventRecord(ev_[1], stream_));
+    DMM_TRY(enqueue_var(false, nullptr));
+    DMM_CUDA(cudaEventRecord(ev_[2], stream_));
+    DMM_CUDA(cudaEventSynchronize(ev_[2]));
+    float a = 0, b = 0;
+    DMM_CUDA(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+    DMM_CUDA(cudaEventElapsedTime(&b, ev_[1], ev_[2]));
+    t->clause_ms += a;
+    t->var_ms += b;
+    t->step_ms += a + b;
+    t->launches += 2;
+  }
+  return DMM_OK;
+}
+
+dmm_status Pack::read_active(int32_t* active) {
+  DMM_CUDA(cudaMemcpyAsync(active, active_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::run(double wall_s, int64_t* steps_launched, bool* timed_out) {
+  DMM_CUDA(cudaSetDevice(dev_));
+  *timed_out = false;
+  if (steps_launched) *steps_launched = 0;
+  if (!pinned_) DMM_CUDA(cudaMallocHost(&pinned_, 2 * sizeof(int32_t)));
+  const auto t0 = std::chrono::steady_clock::now();
+  auto elapsed = [&]() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  };
+  int32_t active = 0;
+  DMM_TRY(read_active(&active));
+  if (active <= 0) return DMM_OK;
+  const int32_t S = tun_.steps_per_graph;
+  int cur = 0;
+  DMM_TRY(launch_steps(S));
+  DMM_CUDA(cudaMemcpyAsync(pinned_ + cur, active_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaEventRecord(ev_[cur], stream_));
+  if (steps_launched) *steps_launched += S;
+  for (;;) {
+    const int nxt = cur ^ 1;
+    DMM_TRY(launch_steps(S));
+    DMM_CUDA(cudaMemcpyAsync(pinned_ + nxt, active_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    DMM_CUDA(cudaEventRecord(ev_[nxt], stream_));
+    if (steps_launched) *steps_launched += S;
+    DMM_CUDA(cudaEventSynchronize(ev_[cur]));
+    if (pinned_[cur] <= 0) break;
+    if (wall_s > 0 && elapsed() > wall_s) {
+      *timed_out = true;
+      break;
+    }
+    cur = nxt;
+  }
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::resume(int32_t idx) {
+  InstCtrl c;
+  DMM_TRY(read_ctrl(idx, &c));
+  if (c.done != DMM_STEP_LIMIT) return DMM_OK;
+  c.done = 0;
+  DMM_TRY(add_active(+1));
+  DMM_TRY(write_ctrl(idx, c));
+  return DMM_OK;
+}
+
+dmm_status Pack::drain_finished(std::vector<int32_t>* out) {
+  out->clear();
+  int32_t tail = 0;
+  DMM_CUDA(cudaMemcpyAsync(&tail, ring_tail_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  if (tail == ring_read_) return DMM_OK;
+  std::vector<int32_t> ring(caps_.insts);
+  DMM_CUDA(cudaMemcpy(ring.data(), ring_d_, caps_.insts * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  for (int32_t p = ring_read_; p < tail; p++) out->push_back(ring[p % caps_.insts]);
+  ring_read_ = tail;
+  return DMM_OK;
+}
+
+dmm_status Pack::stop(int32_t idx, int32_t status) {
+  InstCtrl c;
+  DMM_TRY(read_ctrl(idx, &c));
+  if (c.done != 0) return DMM_OK;
+  c.done = status;
+  DMM_TRY(add_active(-1));
+  DMM_TRY(write_ctrl(idx, c));
+  return DMM_OK;
+}
+
+dmm_status Pack::sync() {
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, double* energy) {
+  if (!live(idx) || !x || !dxdt) return DMM_ERR_ARG;
+  DMM_TRY(set_state(idx, x));
+  const InstDesc& I = inst_h_[idx];
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  // tiles of this instance only
+  std::vector<Tile> ct, vt;
+  for (int32_t b = 0; b < I.m; b += tun_.clause_tile)
+    ct.push_back(Tile{idx, b, std::min(tun_.clause_tile, I.m - b), 0});
+  for (int32_t b = 0; b < I.n; b += tun_.var_tile)
+    vt.push_back(Tile{idx, b, std::min(tun_.var_tile, I.n - b), 0});
+  const int64_t need = std::max<int64_t>(std::max(ct.size(), vt.size()), 1);
+  if (need > aux_cap_) {
+    if (aux_ctiles_d_) DMM_CUDA(cudaFree(aux_ctiles_d_));
+    if (aux_vtiles_d_) DMM_CUDA(cudaFree(aux_vtiles_d_));
+    aux_ctiles_d_ = aux_vtiles_d_ = nullptr;
+    DMM_CUDA(cudaMalloc(&aux_ctiles_d_, need * sizeof(Tile)));
+    DMM_CUDA(cudaMalloc(&aux_vtiles_d_, need * sizeof(Tile)));
+    aux_cap_ = need;
+  }
+  if (!ct.empty())
+    DMM_CUDA(cudaMemcpyAsync(aux_ctiles_d_, ct.data(), ct.size() * sizeof(Tile),
+                             cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaMemcpyAsync(aux_vtiles_d_, vt.data(), vt.size() * sizeof(Tile),
+                           cudaMemcpyHostToDevice, stream_));
+  int32_t nt[2] = {(int32_t)ct.size(), (int32_t)vt.size()};
+  DMM_CUDA(cudaMemcpyAsync(ntiles_d_ + 2, nt, sizeof nt, cudaMemcpyHostToDevice, stream_));
+  // the finalize of a right-hand side reads the epart of the auxiliary tiles
+  InstDesc Iaux = I;
+  Iaux.ctile0 = 0;
+  Iaux.nctile = nt[0];
+  DMM_CUDA(cudaMemcpyAsync(inst_d_ + idx, &Iaux, sizeof(InstDesc), cudaMemcpyHostToDevice, stream_));
+  const int gc = grid_c_, gv = grid_v_;
+  grid_c_ = std::max(1, std::min(nt[0], sms_ * 8));
+  grid_v_ = std::max(1, std::min(nt[1], sms_ * 8));
+  use_aux_ = true;
+  dmm_status st = enqueue_step(true, stage_);
+  use_aux_ = false;
+  grid_c_ = gc;
+  grid_v_ = gv;
+  DMM_TRY(st);
+  if (prec_ == DMM_FP64)
+    k_clause_dx<double><<<blocks_for(I.m), kThreads, 0, stream_>>>(
+        inst_d_, idx, static_cast<double*>(Xs_), static_cast<double*>(Cp_),
+        static_cast<double*>(alpha_cm_), stage_);
+  else
+    k_clause_dx<float><<<blocks_for(I.m), kThreads, 0, stream_>>>(
+        inst_d_, idx, static_cast<float*>(Xs_), static_cast<float*>(Cp_),
+        static_cast<float*>(alpha_cm_), stage_);
+  DMM_CUDA(cudaGetLastError());
+  k_rhs_finish<<<1, kThreads, 0, stream_>>>(inst_d_, ctrl_d_, idx, epart_);
+  DMM_CUDA(cudaGetLastError());
+  DMM_TRY(upload_desc(idx));
+  DMM_CUDA(cudaMemcpyAsync(dxdt, stage_, N * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  InstCtrl c;
+  DMM_TRY(read_ctrl(idx, &c));
+  if (loc) *loc = c.loc;
+  if (energy) *energy = c.energy;
+  return DMM_OK;
+}
+
+dmm_status Pack::dostep(int32_t idx, const double* x, const double* dxdt, double h, double* xo) {
+  if (!live(idx) || !x || !dxdt || !xo) return DMM_ERR_ARG;
+  const InstDesc& I = inst_h_[idx];
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  DMM_TRY(ensure_stage(3 * N));
+  DMM_CUDA(cudaMemcpyAsync(stage_, x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaMemcpyAsync(stage_ + N, dxdt, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  if (prec_ == DMM_FP64)
+    k_dostep<double><<<blocks_for(N), kThreads, 0, stream_>>>(inst_d_, idx, unit_, stage_,
+                                                              stage_ + N, h, stage_ + 2 * N);
+  else
+    k_dostep<float><<<blocks_for(N), kThreads, 0, stream_>>>(inst_d_, idx, unit_, stage_,
+                                                             stage_ + N, h, stage_ + 2 * N);
+  DMM_CUDA(cudaGetLastError());
+  DMM_CUDA(cudaMemcpyAsync(xo, stage_ + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+template <class T>
+static dmm_status signs_of(const T* dV, int32_t n, int8_t* out, bool zero_as_zero, cudaStream_t s) {
+  std::vector<T> h(n);
+  DMM_CUDA(cudaMemcpyAsync(h.data(), dV, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  DMM_CUDA(cudaStreamSynchronize(s));
+  for (int32_t i = 0; i < n; i++)
+    out[i] = h[i] > T(0) ? 1 : ((h[i] < T(0) || !zero_as_zero) ? -1 : 0);
+  return DMM_OK;
+}
+
+dmm_status Pack::assignment(int32_t idx, int8_t* pre, int8_t* post) {
+  if (!live(idx)) return DMM_ERR_ARG;
+  InstCtrl c;
+  DMM_TRY(read_ctrl(idx, &c));
+  const InstDesc& I = inst_h_[idx];
+  auto vptr = [&](int set, int k) -> const void* {
+    return static_cast<const char*>(cand_) +
+           ((int64_t)(set * kTrials + k) * caps_.vars + I.var0) * (int64_t)tsize_;
+  };
+  if (pre) {
+    if (c.solved_step < 0) {
+      set_error("instance %d is not solved", idx);
+      return DMM_ERR_STATE;
+    }
+    if (prec_ == DMM_FP64)
+      DMM_TRY(signs_of(static_cast<const double*>(vptr(c.sol_set, c.sol_k)), I.n, pre, true, stream_));
+    else
+      DMM_TRY(signs_of(static_cast<const float*>(vptr(c.sol_set, c.sol_k)), I.n, pre, true, stream_));
+  }
+  if (post) {
+    if (prec_ == DMM_FP64)
+      DMM_TRY(signs_of(static_cast<const double*>(vptr(c.set, c.kcur)), I.n, post, false, stream_));
+    else
+      DMM_TRY(signs_of(static_cast<const float*>(vptr(c.set, c.kcur)), I.n, post, false, stream_));
+  }
+  return DMM_OK;
+}
+
+}  // namespace dmm

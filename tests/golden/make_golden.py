@@ -1,0 +1,128 @@
+"""Regenerates the golden fixtures from the reference (run in a container that has the
+reference sources; the committed outputs travel with the repository).
+
+    python tests/golden/make_golden.py [--ref-dir /root/reference]
+
+Outputs, next to this script:
+  fixtures.npz        the reference's CNF fixtures n = 100 .. 1000 (cnf/*.cnf) as arrays,
+                      with the planted assignment of their first comment line when present
+  known_answers.json  the UNMODIFIED reference CLI (oracle/_ref/dynex_ref) on each fixture
+                      and seed 0, 1, 2 (plus n = 10000, seed 0): printed step count, T,
+                      and the reported `v` assignment; and the reference's per-step harness
+                      (oracle/_ref/libdynex_ref.so) from a seeded uniform initial state:
+                      SHA-256 of the FP64 state at selected steps, solve step and T.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import hashlib
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.oracle import REF_CLI, Reference, build, read_cnf  # noqa: E402
+
+HASH_STEPS = [0, 1, 2, 3, 5, 10, 20, 50, 100, 150, 200]
+
+
+def uniform_init(n, m, seed):
+    rng = np.random.default_rng(seed)
+    return np.concatenate([rng.uniform(-1, 1, n), rng.uniform(0, 1, m), np.ones(m)])
+
+
+def state_hash(x: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(x, dtype="<f8").tobytes()).hexdigest()
+
+
+def run_cli(path: str, seed: int, timeout: float = 600.0) -> dict:
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, os.path.basename(path))
+        shutil.copy(path, p)
+        out = subprocess.run([REF_CLI, "-i", p, "-l", str(seed)], capture_output=True, text=True,
+                             timeout=timeout, cwd=d).stdout
+    text = out.replace("\r", "\n")
+    # The progress line of the solving right-hand side carries T and the step counter
+    # (dynex.cc:609-636); it is printed before the reference's display thread starts
+    # writing, so it is never interleaved.
+    m = None
+    steps = None
+    for line in text.splitlines():
+        mm = re.search(r"T=([0-9.]+) GLOBAL=.*\(LOC=0\) \((\d+)\)", line)
+        if mm:
+            m, steps = mm, int(mm.group(2))
+            break
+    v = []
+    for line in text.splitlines():
+        if line.startswith("v "):
+            v += [int(t) for t in line[2:].split()]
+    if v and v[-1] == 0:
+        v = v[:-1]
+    return {"solved": m is not None, "T": float(m.group(1)) if m else None, "steps": steps,
+            "v": v}
+
+
+def planted_of(path: str):
+    with open(path) as f:
+        first = f.readline()
+    if first.startswith("c ["):
+        return np.array([1 if int(t) > 0 else -1 for t in first[3:].split("]")[0].split()],
+                        dtype=np.int8)
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-dir", default="/root/reference")
+    a = ap.parse_args()
+    build()
+    paths = sorted(glob.glob(os.path.join(a.ref_dir, "cnf", "*.cnf")),
+                   key=lambda p: int(re.search(r"_n_(\d+)_", p).group(1)))
+    arrays = {}
+    answers = {"cli": {}, "harness": {}}
+    for path in paths:
+        n, m, lits, coff = read_cnf(path)
+        name = f"n{n}"
+        if n <= 1000:
+            arrays[f"{name}_lits"] = lits.astype(np.int16)
+            arrays[f"{name}_off"] = coff.astype(np.int32)
+            pl = planted_of(path)
+            if pl is not None:
+                arrays[f"{name}_planted"] = pl
+            for seed in (0, 1, 2):
+                r = run_cli(path, seed)
+                answers["cli"][f"{name}_seed{seed}"] = r
+                print(name, seed, r["steps"], r["T"], file=sys.stderr)
+            ref = Reference(n, m, lits, coff)
+            x0 = uniform_init(n, m, 1234 + n)
+            res = ref.run(x0, 200, dump_every=1)
+            hashes = {str(s): state_hash(res["dump"][s]) for s in HASH_STEPS
+                      if s < len(res["dump"]) and s <= res["steps"]}
+            answers["harness"][f"{name}_uniform"] = {
+                "init_seed": 1234 + n, "max_steps": 200, "steps": res["steps"],
+                "solved": res["solved"], "solve_step": res["solve_step"],
+                "solve_t": res["solve_t"], "hashes": hashes,
+                "loc": res["loc"][: min(len(res["loc"]), 50)].tolist()}
+        elif n == 10000:
+            r = run_cli(path, 0)
+            answers["cli"][f"{name}_seed0"] = {k: r[k] for k in ("solved", "T", "steps")}
+            answers["cli"][f"{name}_seed0"]["v_sha256"] = hashlib.sha256(
+                np.array(r["v"], dtype="<i4").tobytes()).hexdigest()
+            print(name, 0, r["steps"], r["T"], file=sys.stderr)
+    np.savez_compressed(os.path.join(HERE, "fixtures.npz"), **arrays)
+    with open(os.path.join(HERE, "known_answers.json"), "w") as f:
+        json.dump(answers, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

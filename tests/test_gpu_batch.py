@@ -1,0 +1,156 @@
+"""Batched and served paths: every instance's result is identical alone and in the mix;
+plus full-size (n = 100,000, m = 800,000) checks of the production FP32 path."""
+import numpy as np
+import pytest
+
+import dmm_b200 as dmm
+from conftest import uniform_init
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def formula(f):
+    return dmm.from_arrays(f["lits"], f["off"], f["n"])
+
+
+def alone(form, x0, prec, max_steps):
+    with dmm.Instance(form, precision=prec) as inst:
+        inst.set_state(x0)
+        r = inst.solve(max_steps=max_steps)
+        _, post = inst.assignment(pre=False)
+        return r, post, inst.get_state()[0]
+
+
+def mix(fixtures):
+    items = []
+    for i, name in enumerate(["n100", "n200", "n500", "n1000", "n200", "n100", "n1000", "n500"]):
+        f = fixtures[name]
+        form = formula(f)
+        items.append((form, uniform_init(f["n"], f["m"], 100 + i)))
+    return items
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_batch_results_equal_alone(fixtures, prec):
+    items = mix(fixtures)
+    b = dmm.Batch.for_formulas([f for f, _ in items], precision=prec)
+    for form, x0 in items:
+        b.add(form, x0, max_steps=300)
+    stats = b.run()
+    assert stats["solved"] + stats["unsolved"] == len(items)
+    for k, (form, x0) in enumerate(items):
+        r_b, post_b = b.result(k)
+        x_b, _ = b.state(k)
+        r_a, post_a, x_a = alone(form, x0, prec, 300)
+        assert (r_b.status, r_b.steps, r_b.solved_step, r_b.t, r_b.loc) == (
+            r_a.status, r_a.steps, r_a.solved_step, r_a.t, r_a.loc)
+        assert np.array_equal(post_b, post_a)
+        assert np.array_equal(x_b, x_a)
+
+
+def test_batch_tuning_does_not_change_results(fixtures):
+    items = mix(fixtures)
+    finals = []
+    for kw in (dict(var_group=1, steps_per_graph=8), dict(var_group=32, steps_per_graph=64,
+                                                           clause_tile=2048, var_tile=512)):
+        b = dmm.Batch.for_formulas([f for f, _ in items], precision="fp32")
+        b.set_tuning(**kw)
+        for form, x0 in items:
+            b.add(form, x0, max_steps=120)
+        b.run()
+        finals.append([b.state(k)[0] for k in range(len(items))])
+    for a, c in zip(*finals):
+        assert np.array_equal(a, c)
+
+
+def test_server_results_equal_alone(fixtures):
+    items = mix(fixtures) + mix(fixtures)[:4]
+    srv = dmm.Server(budget_bytes=8 << 20, max_slots=5, steps_per_launch=16, precision="fp32")
+    tickets = {}
+    pending = list(enumerate(items))
+    done = {}
+    rounds = 0
+    while pending or len(done) < len(items):
+        # arrivals interleaved with work on the device
+        for _ in range(2):
+            if pending:
+                k, (form, x0) = pending.pop(0)
+                tickets[srv.submit(form, x0=x0, max_steps=250)] = k
+        srv.pump()
+        for res in srv.take():
+            done[tickets[res["ticket"]]] = res
+        rounds += 1
+        assert rounds < 10000
+    for k, (form, x0) in enumerate(items):
+        r_a, post_a, _ = alone(form, x0, "fp32", 250)
+        r_s = done[k]["result"]
+        assert (r_s.status, r_s.steps, r_s.solved_step, r_s.t) == (
+            r_a.status, r_a.steps, r_a.solved_step, r_a.t)
+        assert np.array_equal(done[k]["assignment"], post_a)
+        assert done[k]["finish_s"] >= done[k]["admit_s"] >= done[k]["submit_s"]
+
+
+def test_server_budget_admission(fixtures):
+    f = fixtures["n1000"]
+    form = formula(f)
+    srv = dmm.Server(budget_bytes=1 << 18, max_slots=4, steps_per_launch=8)
+    with pytest.raises(dmm.DmmError) as e:
+        srv.submit(form, seed=1)
+    assert e.value.name == "DMM_ERR_BUDGET"
+    small = formula(fixtures["n100"])
+    tickets = [srv.submit(small, seed=s, max_steps=40) for s in range(6)]
+    resident, queued = srv.pump()
+    assert resident + queued <= 6 and resident <= 4
+    got = []
+    for _ in range(200):
+        srv.pump()
+        got += srv.take()
+        if len(got) == len(tickets):
+            break
+    assert sorted(r["ticket"] for r in got) == sorted(tickets)
+
+
+@pytest.fixture(scope="module")
+def big():
+    form, planted = dmm.generate_planted(100_000, 800_000, p0=0.08, p1=0.46, seed=2024)
+    return form, planted
+
+
+def test_full_size_fp32_bitexact_vs_oracle_first_steps(big):
+    """n = 100,000, m = 800,000: the first 12 steps equal the oracle's FP32 restatement."""
+    form, _ = big
+    x0 = dmm.initial_state_uniform(form, 77)
+    o = Oracle(form.n, form.m, form.lits, form.clause_off, precision="fp32")
+    ref = o.run(x0, 12, dump_every=4)
+    with dmm.Instance(form, precision="fp32") as inst:
+        inst.set_state(x0)
+        for r in range(1, 4):
+            inst.step(4)
+            assert np.array_equal(inst.get_state()[0], ref["dump"][r])
+
+
+def test_full_size_fp32_properties(big):
+    """Determinism, state bounds and the unsatisfied count against a host recount."""
+    form, planted = big
+    n, m = form.n, form.m
+    x0 = dmm.initial_state_uniform(form, 78)
+    finals = []
+    for _ in range(2):
+        with dmm.Instance(form, precision="fp32") as inst:
+            inst.set_state(x0)
+            rep = inst.step(60)
+            finals.append((inst.get_state()[0], rep))
+    (x, rep), (x2, rep2) = finals
+    assert np.array_equal(x, x2) and rep.t == rep2.t and rep.loc == rep2.loc
+    assert np.all(np.abs(x[:n]) <= 1)
+    assert np.all((x[n:n + m] >= 0) & (x[n:n + m] <= 1)) and np.all(x[n + m:] >= 1)
+    # loc of the right-hand side at the final state, recounted on the host in FP32
+    with dmm.Instance(form, precision="fp32") as inst:
+        _, loc, _ = inst.generate_dxdt(x)
+    v = np.clip(x[:n].astype(np.float32), -1, 1)
+    lits = form.lits.reshape(-1, 3)
+    q = np.sign(lits).astype(np.float32)
+    a = (np.float32(1) - q * v[np.abs(lits) - 1]).min(axis=1) * np.float32(0.5)
+    assert loc == int((a >= 0.5).sum())
+    assert dmm.check_assignment(form, planted) == 0

@@ -1,0 +1,116 @@
+"""The oracle (CPU restatement) pinned against the reference: the golden known answers of
+the unmodified reference CLI and, where the reference harness is built, per-step states."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import uniform_init
+from oracle.oracle import Oracle, Reference, reference_available
+
+FIXTURES = ["n100", "n200", "n500", "n1000"]
+
+
+def state_hash(x):
+    return hashlib.sha256(np.ascontiguousarray(x, dtype="<f8").tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_oracle_matches_reference_cli(fixtures, known_answers, name, seed):
+    """Steps, T and the reported `v` assignment of `dynex -i fixture -l seed`."""
+    f = fixtures[name]
+    o = Oracle(f["n"], f["m"], f["lits"], f["off"])
+    x0 = o.init_state(seed)
+    ka = known_answers["cli"][f"{name}_seed{seed}"]
+    r = o.run(x0, 2000)
+    assert r["solved"]
+    assert r["solve_step"] == ka["steps"]
+    assert round(r["solve_t"], 2) == pytest.approx(ka["T"], abs=1e-9)
+    v = [(i + 1) if a > 0 else -(i + 1) for i, a in enumerate(r["post"])]
+    assert v == ka["v"]
+    assert o.check(r["pre"]) == 0
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_oracle_matches_reference_harness_hashes(fixtures, known_answers, name):
+    """FP64 state after selected steps from a seeded uniform initial state (SHA-256 of the
+    reference's own per-step states)."""
+    f = fixtures[name]
+    ka = known_answers["harness"][f"{name}_uniform"]
+    o = Oracle(f["n"], f["m"], f["lits"], f["off"])
+    x0 = uniform_init(f["n"], f["m"], ka["init_seed"])
+    r = o.run(x0, ka["max_steps"], dump_every=1)
+    assert r["steps"] == ka["steps"]
+    assert r["solved"] == ka["solved"]
+    assert r["solve_step"] == ka["solve_step"]
+    assert r["solve_t"] == ka["solve_t"]
+    for s, h in ka["hashes"].items():
+        assert state_hash(r["dump"][int(s)]) == h, f"step {s}"
+    assert r["loc"][: len(ka["loc"])].tolist() == ka["loc"]
+
+
+def test_oracle_n10000_known_answer(known_answers):
+    """The largest fixture is not committed; its known answer is checked by the GPU tests
+    against generated data only through the CLI table."""
+    ka = known_answers["cli"]["n10000_seed0"]
+    assert ka["steps"] == 156 and ka["T"] == 13.62
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("name", ["n100", "n200"])
+def test_oracle_bitexact_vs_reference_per_step(fixtures, name):
+    f = fixtures[name]
+    o = Oracle(f["n"], f["m"], f["lits"], f["off"])
+    ref = Reference(f["n"], f["m"], f["lits"], f["off"])
+    for seed in (3, 4):
+        x0 = uniform_init(f["n"], f["m"], seed)
+        a = o.run(x0, 150, dump_every=1)
+        b = ref.run(x0, 150, dump_every=1)
+        assert np.array_equal(a["dump"], b["dump"])
+        assert np.array_equal(a["loc"], b["loc"])
+        assert np.array_equal(a["energy"], b["energy"])
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference harness not built")
+def test_oracle_general_ksat_vs_reference():
+    """Mixed clause sizes (unit, 2-, 3-, k-literal up to 25, repeated variables)."""
+    rng = np.random.default_rng(7)
+    n = 60
+    lits, off = [], [0]
+    for c in range(400):
+        k = int(rng.choice([1, 2, 3, 3, 3, 4, 5, 7, 12, 25])) if c % 50 else 1
+        vs = rng.integers(1, n + 1, size=k)
+        sg = rng.choice([-1, 1], size=k)
+        lits += list(vs * sg)
+        off.append(len(lits))
+    lits = np.array(lits, np.int32)
+    off = np.array(off, np.int64)
+    o = Oracle(n, len(off) - 1, lits, off)
+    ref = Reference(n, len(off) - 1, lits, off)
+    x0 = o.init_state(5)
+    a = o.run(x0, 120, dump_every=1)
+    b = ref.run(x0, 120, dump_every=1)
+    assert np.array_equal(a["dump"], b["dump"])
+    d1, l1, e1 = o.rhs(a["dump"][7])
+    d2, l2, e2 = ref.rhs(a["dump"][7])
+    assert np.array_equal(d1, d2) and l1 == l2 and e1 == e2
+
+
+def test_oracle_fp32_mode_tracks_fp64(fixtures):
+    """FP32 production mode stays close to FP64 over a short horizon."""
+    f = fixtures["n200"]
+    o64 = Oracle(f["n"], f["m"], f["lits"], f["off"])
+    o32 = Oracle(f["n"], f["m"], f["lits"], f["off"], precision="fp32")
+    x0 = uniform_init(f["n"], f["m"], 11)
+    a = o64.run(x0, 10, dump_every=1)
+    b = o32.run(x0, 10, dump_every=1)
+    n = f["n"]
+    assert np.max(np.abs(a["dump"][10][:n] - b["dump"][10][:n])) < 1e-3
+
+
+def test_oracle_planted_fixtures_verify(fixtures):
+    for name in ("n200", "n500", "n1000"):
+        f = fixtures[name]
+        o = Oracle(f["n"], f["m"], f["lits"], f["off"])
+        assert o.check(f["planted"]) == 0
