@@ -1,0 +1,244 @@
+// dynex: drop-in command line of the reference solver (dynex.cc:2204-2296, report
+// dynex.cc:1480-1533 and 662-703), running the integrator on the GPU through libdmm.
+//
+//   dynex -i file.cnf [-l seed] [-w replicas] [-u walltime] [-z maxsteps]
+//         [-c alpha] [-b beta] [-n gamma] [-h delta] [-j epsilon] [-k zeta] [-m xl_max]
+//         [-q 0|1] [-P fp64|fp32] [-D device]
+//
+// Defaults follow the reference (FP64 arithmetic, seed 0, one replica); with them the
+// reported step count, T and assignment equal the reference's.  -P fp32 selects the
+// production FP32 path.  Replicas (-w) start from the reference's per-replica initial
+// states with alpha / i (dynex.cc:2643-2700) and run together in one batch; the replica
+// that solves at the lowest step wins.  Options of the reference that select modes
+// outside the default integrator (-o, -t, -p, -e, ...) are accepted and reported as
+// unsupported when they ask for anything but the default.
+#include <getopt.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dmm.h"
+
+namespace {
+
+struct Opts {
+  std::string input;
+  int seed = 0;
+  int replicas = 1;
+  double walltime = 0.0;
+  int max_steps = 0;
+  bool quiet = false;
+  dmm_precision prec = DMM_FP64;
+  int device = 0;
+  dmm_params p{};
+};
+
+void usage(const char* argv0) {
+  std::printf("c Syntax: %s -i file.cnf [options]\n", argv0);
+  std::printf(
+      "c   -i file     input CNF (DIMACS)\n"
+      "c   -l int      seed (0: replica 0 starts at 1.0; other seeds: V in {-1,0,1})\n"
+      "c   -w int      replicas run together on the GPU (reference: threads)\n"
+      "c   -u sec      wall-time limit\n"
+      "c   -z int      accepted-step limit\n"
+      "c   -c -b -n -h -j -k float   alpha beta gamma delta epsilon zeta\n"
+      "c   -m int      Xl bound factor (bound = factor * m)\n"
+      "c   -q 0|1      quiet\n"
+      "c   -P fp64|fp32  arithmetic (default fp64, the reference's)\n"
+      "c   -D int      CUDA device\n");
+}
+
+bool fail(dmm_status st, const char* what) {
+  if (st == DMM_OK) return false;
+  std::fprintf(stderr, "c ERROR: %s: %s (%s)\n", what, dmm_status_string(st), dmm_last_error());
+  return true;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Opts o;
+  dmm_params_default(&o.p);
+  int c;
+  while ((c = getopt(argc, argv, "i:l:w:u:z:c:b:n:h:j:k:m:q:P:D:o:t:p:e:f:g:r:v:x:y:d:a:s:")) != -1) {
+    const char* a = optarg;
+    if (a && a[0] == '=') a++;  // the reference accepts -x=value (dynex.cc:2208)
+    switch (c) {
+      case 'i': o.input = a; break;
+      case 'l': o.seed = std::atoi(a); break;
+      case 'w': o.replicas = std::atoi(a); break;
+      case 'u': o.walltime = std::atof(a); break;
+      case 'z': o.max_steps = std::atoi(a); break;
+      case 'c': o.p.alpha = std::atof(a); break;
+      case 'b': o.p.beta = std::atof(a); break;
+      case 'n': o.p.gamma = std::atof(a); break;
+      case 'h': o.p.delta = std::atof(a); break;
+      case 'j': o.p.epsilon = std::atof(a); break;
+      case 'k': o.p.zeta = std::atof(a); break;
+      case 'm': o.p.xl_max = std::atoi(a); break;
+      case 'q': o.quiet = std::atoi(a) != 0; break;
+      case 'P': o.prec = std::strcmp(a, "fp32") == 0 ? DMM_FP32 : DMM_FP64; break;
+      case 'D': o.device = std::atoi(a); break;
+      case 'o':
+        if (std::atoi(a) != 6) std::fprintf(stderr, "c -o %s: only the default integrator (6) is available\n", a);
+        break;
+      case 't':
+        if (std::atoi(a) != 0) std::fprintf(stderr, "c -t %s: tuning mode is not available\n", a);
+        break;
+      case 'p':
+        if (std::atoi(a) != 0) std::fprintf(stderr, "c -p %s: alpha heuristics are not available\n", a);
+        break;
+      default:
+        break;  // other reference options only affect modes outside the default path
+    }
+  }
+  if (o.input.empty() || o.replicas < 1) {
+    usage(argv[0]);
+    return EXIT_FAILURE;
+  }
+  dmm_cnf* cnf = nullptr;
+  dmm_status st = dmm_cnf_read(o.input.c_str(), &cnf);
+  if (st != DMM_OK) {
+    if (st == DMM_ERR_CLAUSE_LEN) std::printf("c ERROR: %s\n", dmm_last_error());
+    else fail(st, "reading the formula");
+    return EXIT_FAILURE;
+  }
+  const int n = cnf->n, m = cnf->m;
+  if (!o.quiet) {
+    std::printf("c --------------------------------------------\n");
+    std::printf("c DMM INTEGRATOR ON B200 (sm_100a)\n");
+    std::printf("c --------------------------------------------\n");
+    std::printf("c INSTANCE  : %s\n", o.input.c_str());
+    std::printf("c VARIABLES : %d\n", n);
+    std::printf("c CLAUSES   : %d\n", m);
+    std::printf("c RATIO     : %lf\n", (double)m / n);
+    std::printf("c MAX VARIABLE OCCURENCE: %d\n", cnf->max_occurrence);
+    std::printf("c PRECISION : %s\n", o.prec == DMM_FP64 ? "FP64" : "FP32");
+    std::printf("c REPLICAS  : %d\n", o.replicas);
+    std::printf("c ALPHA %.15f BETA %.15f GAMMA %.15f DELTA %.15f EPSILON %.15f ZETA %.15f\n",
+                o.p.alpha, o.p.beta, o.p.gamma, o.p.delta, o.p.epsilon, o.p.zeta);
+    std::printf("c SEED      : %d\n", o.seed);
+  }
+  const int64_t N = (int64_t)n + 2 * (int64_t)m;
+  std::vector<double> x(N);
+  const double t0 = now_s();
+  dmm_report rep{};
+  std::vector<int8_t> pre(n), post(n);
+  int winner = 0;
+  bool solved = false;
+  if (o.replicas == 1) {
+    dmm_instance* inst = nullptr;
+    int32_t div = 1;
+    if (fail(dmm_instance_create(cnf->lits, cnf->clause_off, n, m, o.prec, o.device, &inst),
+             "creating the instance") ||
+        fail(dmm_initial_state_reference(cnf->lits, cnf->clause_off, n, m, o.seed, 0, x.data(), &div),
+             "initial state") ||
+        fail(dmm_instance_set_params(inst, &o.p, nullptr), "parameters") ||
+        fail(dmm_instance_set_state(inst, x.data()), "state")) {
+      dmm_instance_destroy(inst);
+      dmm_cnf_free(cnf);
+      return EXIT_FAILURE;
+    }
+    if (!o.quiet) std::printf("c [0] STARTING ODE...\n");
+    dmm_limits lim{o.max_steps, 0, o.walltime};
+    if (fail(dmm_instance_solve(inst, &lim, &rep), "integration")) {
+      dmm_instance_destroy(inst);
+      dmm_cnf_free(cnf);
+      return EXIT_FAILURE;
+    }
+    solved = rep.status == DMM_SOLVED;
+    if (fail(dmm_instance_assignment(inst, solved ? pre.data() : nullptr, post.data()),
+             "assignment")) {
+      dmm_instance_destroy(inst);
+      dmm_cnf_free(cnf);
+      return EXIT_FAILURE;
+    }
+    dmm_instance_destroy(inst);
+  } else {
+    dmm_batch* b = nullptr;
+    const int R = o.replicas;
+    if (fail(dmm_batch_create(o.prec, o.device, R, (int64_t)n * R, (int64_t)m * R,
+                              cnf->nlits * R, &b), "creating the batch")) {
+      dmm_cnf_free(cnf);
+      return EXIT_FAILURE;
+    }
+    for (int r = 0; r < R; r++) {
+      int32_t div = 1, idx = 0;
+      dmm_params pr = o.p;
+      if (fail(dmm_initial_state_reference(cnf->lits, cnf->clause_off, n, m, o.seed, r, x.data(), &div),
+               "initial state"))
+        return EXIT_FAILURE;
+      pr.alpha = o.p.alpha / div;  // dynex.cc:2657
+      if (fail(dmm_batch_add(b, cnf->lits, cnf->clause_off, n, m, &pr, x.data(), o.max_steps, &idx),
+               "adding a replica"))
+        return EXIT_FAILURE;
+    }
+    if (!o.quiet) std::printf("c [*] STARTING ODE ON %d REPLICAS...\n", R);
+    dmm_batch_stats stats{};
+    if (fail(dmm_batch_run_until(b, o.walltime, 1, &stats), "integration")) return EXIT_FAILURE;
+    int best = -1;
+    dmm_report rr{};
+    for (int r = 0; r < R; r++) {
+      dmm_batch_result(b, r, &rr, nullptr);
+      if (rr.status == DMM_SOLVED && (best < 0 || rr.solved_step < rep.solved_step)) {
+        best = r;
+        rep = rr;
+      }
+    }
+    if (best < 0) {
+      dmm_batch_result(b, 0, &rep, nullptr);
+      best = 0;
+    }
+    winner = best;
+    solved = rep.status == DMM_SOLVED;
+    dmm_batch_assignment(b, best, solved ? pre.data() : nullptr, post.data());
+    dmm_batch_destroy(b);
+  }
+  const double spent = now_s() - t0;
+  if (solved) {
+    std::printf("\nc [%d] T=%.2f SOLUTION FOUND\n", winner, rep.solved_t);
+    for (int i = 0; i < n; i++)
+      if (pre[i] != 0) std::printf("%d ", pre[i] > 0 ? i + 1 : -(i + 1));
+    std::printf("\nc [%d] VERIFYING...\n", winner);
+    const int64_t bad = dmm_check_assignment(cnf->lits, cnf->clause_off, m, n, pre.data());
+    if (bad == 0) {
+      std::printf("c [%d] SAT (VERIFIED)\n", winner);
+      const std::string sol = o.input + ".solution.txt";
+      if (FILE* f = std::fopen(sol.c_str(), "w")) {
+        for (int i = 0; i < n; i++) std::fprintf(f, "%d, ", pre[i] >= 0 ? i + 1 : -(i + 1));
+        std::fclose(f);
+      }
+    } else {
+      std::printf("c [%d] UNSAT (VERIFIED)\n", winner);
+    }
+  }
+  if (!o.quiet) {
+    std::printf("c [%d] TIME SPENT: %.5fs\n", winner, spent);
+    std::printf("c [%d] STEPS = %d (T = %.5f)\n", winner, solved ? rep.solved_step : rep.steps,
+                solved ? rep.solved_t : rep.t);
+    std::printf("c [%d] BEST LOC = %d (GLOBAL %d) **\n", winner, rep.best_loc, rep.best_loc);
+  }
+  if (solved) {
+    std::printf("\ns [%d] SATISFIABLE", winner);
+    for (int i = 0; i < n; i++) {
+      if (i % 20 == 0) std::printf("\nv ");
+      std::printf("%i ", post[i] > 0 ? (i + 1) : -(i + 1));
+    }
+    std::printf("0\n");
+  } else {
+    std::printf("\ns [%d] UNKNOWN\n", winner);
+  }
+  std::printf("%d", solved ? 0 : rep.best_loc);
+  std::fflush(stdout);
+  dmm_cnf_free(cnf);
+  return EXIT_SUCCESS;
+}

@@ -307,8 +307,13 @@ dmm_status dmm_batch_add(dmm_batch* b, const int32_t* lits, const int64_t* claus
 }
 
 dmm_status dmm_batch_run(dmm_batch* b, double wall_s, dmm_batch_stats* stats) {
+  return dmm_batch_run_until(b, wall_s, 0, stats);
+}
+
+dmm_status dmm_batch_run_until(dmm_batch* b, double wall_s, int32_t stop_after,
+                               dmm_batch_stats* stats) {
   dmm::clear_error();
-  if (!b) return DMM_ERR_ARG;
+  if (!b || stop_after < 0) return DMM_ERR_ARG;
   if (b->dirty) {
     DMM_TRY(b->pack->commit_tiles());
     b->dirty = false;
@@ -322,7 +327,7 @@ dmm_status dmm_batch_run(dmm_batch* b, double wall_s, dmm_batch_stats* stats) {
   DMM_CUDA(cudaEventRecord(e0, b->pack->stream()));
   bool timed_out = false;
   int64_t launched = 0;
-  dmm_status st = b->pack->run(wall_s, &launched, &timed_out);
+  dmm_status st = b->pack->run(wall_s, &launched, &timed_out, stop_after);
   DMM_CUDA(cudaEventRecord(e1, b->pack->stream()));
   DMM_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
@@ -333,9 +338,12 @@ dmm_status dmm_batch_run(dmm_batch* b, double wall_s, dmm_batch_stats* stats) {
   const double wall = now_s() - t0;
   std::vector<InstCtrl> after;
   DMM_TRY(b->pack->read_ctrls(&after));
-  if (timed_out)
+  if (timed_out || stop_after > 0)
     for (int32_t i : b->idx)
-      if (after[i].done == 0) DMM_TRY(b->pack->stop(i, DMM_TIME_LIMIT));
+      if (after[i].done == 0) {
+        DMM_TRY(b->pack->stop(i, timed_out ? DMM_TIME_LIMIT : DMM_CANCELLED));
+        after[i].done = timed_out ? DMM_TIME_LIMIT : DMM_CANCELLED;
+      }
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
     for (size_t k = 0; k < b->idx.size(); k++) {
@@ -362,6 +370,12 @@ dmm_status dmm_batch_result(dmm_batch* b, int32_t index, dmm_report* rep, int8_t
   }
   if (post) DMM_TRY(b->pack->assignment(i, nullptr, post));
   return DMM_OK;
+}
+
+dmm_status dmm_batch_assignment(dmm_batch* b, int32_t index, int8_t* pre, int8_t* post) {
+  dmm::clear_error();
+  if (!b || index < 0 || index >= (int32_t)b->idx.size()) return DMM_ERR_ARG;
+  return b->pack->assignment(b->idx[index], pre, post);
 }
 
 dmm_status dmm_batch_state(dmm_batch* b, int32_t index, double* x, double* t) {

@@ -104,9 +104,10 @@ class Pack {
   // after writing flush_bytes of scratch (cold L2); accumulates into *t after sync.
   dmm_status profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t);
   dmm_status read_active(int32_t* active);
-  // Launches step chunks until no instance is running or wall_s (> 0) seconds pass; keeps
-  // one chunk in flight while checking the previous one.  *timed_out tells which.
-  dmm_status run(double wall_s, int64_t* steps_launched, bool* timed_out);
+  // Launches step chunks until no instance is running, or wall_s (> 0) seconds pass, or
+  // (stop_after > 0) that many instances finished during the call; keeps one chunk in
+  // flight while checking the previous one.  *timed_out tells whether time ran out.
+  dmm_status run(double wall_s, int64_t* steps_launched, bool* timed_out, int32_t stop_after = 0);
   // Makes an instance stopped by its step cap runnable again.
   dmm_status resume(int32_t idx);
   // Finished instance indices since the last call.

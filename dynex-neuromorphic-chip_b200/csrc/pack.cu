@@ -815,32 +815,41 @@ dmm_status Pack::read_active(int32_t* active) {
   return DMM_OK;
 }
 
-dmm_status Pack::run(double wall_s, int64_t* steps_launched, bool* timed_out) {
+dmm_status Pack::run(double wall_s, int64_t* steps_launched, bool* timed_out,
+                     int32_t stop_after) {
   DMM_CUDA(cudaSetDevice(dev_));
   *timed_out = false;
   if (steps_launched) *steps_launched = 0;
-  if (!pinned_) DMM_CUDA(cudaMallocHost(&pinned_, 2 * sizeof(int32_t)));
+  if (!pinned_) DMM_CUDA(cudaMallocHost(&pinned_, 4 * sizeof(int32_t)));
   const auto t0 = std::chrono::steady_clock::now();
   auto elapsed = [&]() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   };
-  int32_t active = 0;
+  int32_t active = 0, tail0 = 0;
   DMM_TRY(read_active(&active));
+  DMM_CUDA(cudaMemcpyAsync(&tail0, ring_tail_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
   if (active <= 0) return DMM_OK;
   const int32_t S = tun_.steps_per_graph;
+  // chunk k: S steps, then copies of the running count and the finished-ring tail
+  auto chunk = [&](int slot) -> dmm_status {
+    DMM_TRY(launch_steps(S));
+    DMM_CUDA(cudaMemcpyAsync(pinned_ + slot, active_d_, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             stream_));
+    DMM_CUDA(cudaMemcpyAsync(pinned_ + 2 + slot, ring_tail_d_, sizeof(int32_t),
+                             cudaMemcpyDeviceToHost, stream_));
+    DMM_CUDA(cudaEventRecord(ev_[slot], stream_));
+    if (steps_launched) *steps_launched += S;
+    return DMM_OK;
+  };
   int cur = 0;
-  DMM_TRY(launch_steps(S));
-  DMM_CUDA(cudaMemcpyAsync(pinned_ + cur, active_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
-  DMM_CUDA(cudaEventRecord(ev_[cur], stream_));
-  if (steps_launched) *steps_launched += S;
+  DMM_TRY(chunk(cur));
   for (;;) {
     const int nxt = cur ^ 1;
-    DMM_TRY(launch_steps(S));
-    DMM_CUDA(cudaMemcpyAsync(pinned_ + nxt, active_d_, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
-    DMM_CUDA(cudaEventRecord(ev_[nxt], stream_));
-    if (steps_launched) *steps_launched += S;
+    DMM_TRY(chunk(nxt));
     DMM_CUDA(cudaEventSynchronize(ev_[cur]));
     if (pinned_[cur] <= 0) break;
+    if (stop_after > 0 && pinned_[2 + cur] - tail0 >= stop_after) break;
     if (wall_s > 0 && elapsed() > wall_s) {
       *timed_out = true;
       break;

@@ -129,7 +129,9 @@ SIGNATURES = {
     "dmm_batch_set_tuning": (_i32, [_vp, _P(Tuning)]),
     "dmm_batch_add": (_i32, [_vp, _pi32, _pi64, _i32, _i32, _P(Params), _pd, _i32, _pi32]),
     "dmm_batch_run": (_i32, [_vp, _d, _P(BatchStats)]),
+    "dmm_batch_run_until": (_i32, [_vp, _d, _i32, _P(BatchStats)]),
     "dmm_batch_result": (_i32, [_vp, _i32, _P(Report), _pi8]),
+    "dmm_batch_assignment": (_i32, [_vp, _i32, _pi8, _pi8]),
     "dmm_batch_state": (_i32, [_vp, _i32, _pd, _pd]),
     "dmm_server_create": (_i32, [_P(ServerConfig), _P(_vp)]),
     "dmm_server_destroy": (None, [_vp]),

@@ -235,7 +235,15 @@ dmm_status dmm_batch_add(dmm_batch* b, const int32_t* lits, const int64_t* claus
                          int32_t max_steps, int32_t* index);
 /* Integrates every instance until each is solved or hits its limit (or wall_s passes). */
 dmm_status dmm_batch_run(dmm_batch* b, double wall_s, dmm_batch_stats* stats);
+/* Like dmm_batch_run, but returns once at least stop_after instances have finished
+ * (solved or at their step cap) during this call; instances still running are stopped
+ * with DMM_CANCELLED.  Replaces the reference's replica race (`-w`, dynex.cc:2738-2801:
+ * the first replica to solve ends the run). */
+dmm_status dmm_batch_run_until(dmm_batch* b, double wall_s, int32_t stop_after,
+                               dmm_batch_stats* stats);
 dmm_status dmm_batch_result(dmm_batch* b, int32_t index, dmm_report* rep, int8_t* post);
+/* Assignments of one instance, as dmm_instance_assignment. */
+dmm_status dmm_batch_assignment(dmm_batch* b, int32_t index, int8_t* pre, int8_t* post);
 dmm_status dmm_batch_state(dmm_batch* b, int32_t index, double* x, double* t);
 
 /* ---- continuous-batching server ------------------------------------------------------- */
