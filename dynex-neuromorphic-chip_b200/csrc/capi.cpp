@@ -251,6 +251,13 @@ dmm_status dmm_instance_time_steps(dmm_instance* inst, int32_t nsteps, double* m
   return st;
 }
 
+dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
+                                           int64_t flush_bytes, double* ms) {
+  dmm::clear_error();
+  if (!inst || nsteps < 0 || flush_bytes < 0 || !ms) return DMM_ERR_ARG;
+  return inst->pack->time_steps_flushed(nsteps, flush_bytes, ms);
+}
+
 // ---- batch ---------------------------------------------------------------------------------
 
 dmm_status dmm_batch_create(dmm_precision precision, int32_t device, int32_t max_instances,

@@ -86,6 +86,8 @@ struct PackView {
   int32_t* ring;            // finished instances (ring buffer)
   int32_t* ring_tail;
   int32_t ring_cap;
+  const int32_t* live;      // indices of the instances with tiles
+  const int32_t* nlive;
 };
 
 // ---- exactly rounded arithmetic (no FMA contraction: the reference has none) ----------

@@ -176,161 +176,6 @@ __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int
   return C;
 }
 
-struct TileSnap {
-  int32_t done, pending, set, kcur;
-  double h;
-};
-
-// Clause tiles.  Per tile: one InstDesc and one control snapshot in shared memory.
-template <class T, bool VEC>
-__global__ void __launch_bounds__(kThreads) k_clause(PackView<T> P) {
-  __shared__ InstDesc s_inst;
-  __shared__ TileSnap s_snap;
-  __shared__ Tile s_tile;
-  __shared__ int s_ti;
-  __shared__ double s_red[kThreads / 32];
-  __shared__ int s_cnt[2][kThreads / 32];
-  if (blockIdx.x == 0 && threadIdx.x == 0) P.queue[1] = 0;  // variable-tile queue is idle
-  const int ntiles = P.ntiles[0];
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const int ti = atomicAdd(&P.queue[0], 1);
-      s_ti = ti;
-      if (ti < ntiles) {
-        s_tile = P.ctiles[ti];
-        s_inst = P.inst[s_tile.inst];
-        const InstCtrl* S = P.ctrl + s_tile.inst;
-        s_snap.done = S->done;
-        s_snap.pending = S->pending;
-        s_snap.set = S->set;
-        s_snap.kcur = S->kcur;
-        s_snap.h = S->h_state;
-      }
-    }
-    __syncthreads();
-    const int ti = s_ti;
-    if (ti >= ntiles) break;
-    if (s_snap.done == 0) {
-      const InstDesc& I = s_inst;
-      const ClauseConsts<T> kc = make_consts<T>(I, s_snap.h);
-      const bool pending = s_snap.pending != 0;
-      const T* __restrict__ V =
-          P.cand + (int64_t)(s_snap.set * kTrials + s_snap.kcur) * P.var_cap + I.var0;
-      T* __restrict__ Xs = P.Xs + I.cls0;
-      T* __restrict__ Xl = P.Xl + I.cls0;
-      T* __restrict__ Cp = P.Cp + I.cls0;
-      const T* __restrict__ acm = I.has_alpha_cm ? P.alpha_cm + I.cls0 : nullptr;
-      const int32_t* __restrict__ lit = P.lit + I.slot0;
-      T* __restrict__ u = P.u + I.slot0;
-      const int c_begin = s_tile.begin, c_end = s_tile.begin + s_tile.count;
-      int unsat = 0, vfail = 0;
-      double e = 0.0;
-      auto one_clause = [&](int c) {
-        T xs = Xs[c], xl = Xl[c];
-        const T al = acm ? acm[c] : kc.alpha;
-        if (pending) advance_memory(xs, xl, Cp[c], al, kc);
-        bool ss;
-        T C;
-        if (I.k3) {
-          const int l0 = __ldg(lit + 3 * c), l1 = __ldg(lit + 3 * c + 1),
-                    l2 = __ldg(lit + 3 * c + 2);
-          T u0, u1, u2;
-          C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1], xs, xl, kc,
-                      u0, u1, u2, ss);
-          u[3 * c] = u0;
-          u[3 * c + 1] = u1;
-          u[3 * c + 2] = u2;
-        } else {
-          const int s0 = P.coff[I.cls0 + c];
-          const int s1 = (c + 1 < I.m) ? P.coff[I.cls0 + c + 1] : I.nslots;
-          C = clause_general(lit + s0, s1 - s0, V, xs, xl, kc, u + s0, ss);
-        }
-        Xs[c] = xs;
-        Xl[c] = xl;
-        Cp[c] = C;
-        unsat += !(C < T(0.5));
-        vfail += !ss;
-        e += (double)C;
-      };
-      auto generic_loop = [&]() {
-        for (int c = c_begin + threadIdx.x; c < c_end; c += kThreads) one_clause(c);
-      };
-      if constexpr (!VEC) {
-        generic_loop();
-      } else if (!I.k3) {
-        generic_loop();
-      } else {
-        // 4 consecutive clauses per thread: 16-byte loads of 12 literals, Xs, Xl, C, and
-        // 16-byte stores of 12 contributions.
-        for (int g = c_begin + 4 * threadIdx.x; g < c_end; g += 4 * kThreads) {
-          if (g + 4 <= c_end) {
-            const int4* L4 = reinterpret_cast<const int4*>(lit + 3 * g);
-            const int4 A = __ldg(L4), B = __ldg(L4 + 1), Cc = __ldg(L4 + 2);
-            const int L[12] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w, Cc.x, Cc.y, Cc.z, Cc.w};
-            const float4 xs4 = *reinterpret_cast<const float4*>(Xs + g);
-            const float4 xl4 = *reinterpret_cast<const float4*>(Xl + g);
-            float4 cp4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (pending) cp4 = *reinterpret_cast<const float4*>(Cp + g);
-            float4 al4 = make_float4(kc.alpha, kc.alpha, kc.alpha, kc.alpha);
-            if (acm) al4 = *reinterpret_cast<const float4*>(acm + g);
-            float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w};
-            float xl[4] = {xl4.x, xl4.y, xl4.z, xl4.w};
-            const float cp[4] = {cp4.x, cp4.y, cp4.z, cp4.w};
-            const float al[4] = {al4.x, al4.y, al4.z, al4.w};
-            float uu[12], cc[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-              if (pending) advance_memory(xs[i], xl[i], T(cp[i]), T(al[i]), kc);
-              bool ss;
-              const int l0 = L[3 * i], l1 = L[3 * i + 1], l2 = L[3 * i + 2];
-              T u0, u1, u2;
-              const T C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1],
-                                  T(xs[i]), T(xl[i]), kc, u0, u1, u2, ss);
-              uu[3 * i] = u0;
-              uu[3 * i + 1] = u1;
-              uu[3 * i + 2] = u2;
-              cc[i] = C;
-              unsat += !(C < T(0.5));
-              vfail += !ss;
-              e += (double)C;
-            }
-            float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
-            U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
-            U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
-            U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
-            *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
-            *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
-            *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
-          } else {
-            for (int c = g; c < c_end; c++) one_clause(c);
-          }
-        }
-      }
-      // unsatisfied / strict-fail counts by ballot+popc, then over warps
-      const int w = threadIdx.x >> 5;
-      unsat = warp_sum_i(unsat);
-      vfail = warp_sum_i(vfail);
-      if ((threadIdx.x & 31) == 0) {
-        s_cnt[0][w] = unsat;
-        s_cnt[1][w] = vfail;
-      }
-      const double et = block_sum_d(e, s_red);
-      if (threadIdx.x == 0) {
-        int tu = 0, tv = 0;
-        for (int i = 0; i < kThreads / 32; i++) {
-          tu += s_cnt[0][i];
-          tv += s_cnt[1][i];
-        }
-        InstCtrl* S = P.ctrl + s_tile.inst;
-        if (tu) atomicAdd(&S->acc_loc, tu);
-        if (tv) atomicAdd(&S->acc_vfail, tv);
-        P.epart[ti] = et;
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // ---- per-variable reduction ---------------------------------------------------------------
 
 // Canonical FP32/FP64 sum of d contributions with G lanes per variable.  Virtual lane
@@ -467,156 +312,6 @@ __device__ __forceinline__ double sorted_sum(const double* __restrict__ u,
   if (d <= 128) return sorted_sum_reg<4>(u, vs, d, lane);
   if (d <= 256) return sorted_sum_reg<8>(u, vs, d, lane);
   return sorted_sum_select(u, vs, d, lane);
-}
-
-// Finalize one instance's step (run by the whole block of its last variable tile).
-template <class T>
-__device__ void finalize_step(const PackView<T>& P, const InstDesc& I, int ii, double* red) {
-  double e = 0.0;
-  for (int i = threadIdx.x; i < I.nctile; i += kThreads) e = __dadd_rn(e, P.epart[I.ctile0 + i]);
-  e = block_sum_d(e, red);
-  if (threadIdx.x == 0) {
-    InstCtrl* S = P.ctrl + ii;
-    volatile InstCtrl* vS = S;
-    const int loc = vS->acc_loc;
-    const int vfail = vS->acc_vfail;
-    const int kmax = vS->acc_kmax;
-    S->loc = loc;
-    S->vfail = vfail;
-    S->energy = e;
-    if (loc < S->best_loc) {
-      S->best_loc = loc;
-      S->best_t = S->t;
-    }
-    const bool solved = (loc == 0 && vfail == 0);
-    if (solved) {
-      S->solved_step = S->step;
-      S->solved_t = S->t;
-      S->sol_set = S->set;
-      S->sol_k = S->kcur;
-    }
-    const int kacc = kmax < kTrials - 1 ? kmax : kTrials - 1;
-    const double hs = 0.125 / (double)(1 << kacc);
-    const double ht = kmax < kTrials ? hs : 0.0078125;
-    S->t = __dadd_rn(S->t, ht);
-    S->step += 1;
-    S->set ^= 1;
-    S->kcur = kacc;
-    S->h_state = hs;
-    S->pending = 1;
-    S->acc_loc = 0;
-    S->acc_vfail = 0;
-    S->acc_kmax = 0;
-    S->vtiles_done = 0;
-    int st = 0;
-    if (solved) st = 1;
-    else if (I.max_steps > 0 && S->step >= I.max_steps) st = 2;
-    if (st) {
-      S->done = st;
-      atomicSub(P.active, 1);
-      const int pos = atomicAdd(P.ring_tail, 1);
-      P.ring[pos % P.ring_cap] = ii;
-    }
-    __threadfence();
-  }
-}
-
-// Variable tiles.  MODE 0: integration step.  MODE 1: right-hand side only (writes dV).
-template <class T, int G, bool SORTED, int MODE>
-__global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restrict__ dv_out) {
-  __shared__ InstDesc s_inst;
-  __shared__ TileSnap s_snap;
-  __shared__ Tile s_tile;
-  __shared__ int s_ti, s_last;
-  __shared__ int s_km[kThreads / 32];
-  __shared__ double s_red[kThreads / 32];
-  if (blockIdx.x == 0 && threadIdx.x == 0) P.queue[0] = 0;  // clause-tile queue is idle
-  const int ntiles = P.ntiles[1];
-  constexpr int VPP = kThreads / G;
-  const int grp = threadIdx.x / G, lane = threadIdx.x % G;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const int ti = atomicAdd(&P.queue[1], 1);
-      s_ti = ti;
-      if (ti < ntiles) {
-        s_tile = P.vtiles[ti];
-        s_inst = P.inst[s_tile.inst];
-        const InstCtrl* S = P.ctrl + s_tile.inst;
-        s_snap.done = S->done;
-        s_snap.set = S->set;
-        s_snap.kcur = S->kcur;
-      }
-    }
-    __syncthreads();
-    const int ti = s_ti;
-    if (ti >= ntiles) break;
-    if (s_snap.done == 0) {
-      const InstDesc& I = s_inst;
-      const T* __restrict__ u = P.u + I.slot0;
-      const int32_t* __restrict__ vsl = P.vslot + I.slot0;
-      const int32_t* __restrict__ vend = P.vend + I.var0;
-      T* __restrict__ cur = P.cand + (int64_t)(s_snap.set * kTrials + s_snap.kcur) * P.var_cap + I.var0;
-      T* __restrict__ nxt = P.cand + (int64_t)((s_snap.set ^ 1) * kTrials) * P.var_cap + I.var0;
-      const int8_t* __restrict__ unit = P.unit + I.var0;
-      const int v_end = s_tile.begin + s_tile.count;
-      int kmax = 0;
-      for (int vb = s_tile.begin; vb < v_end; vb += VPP) {
-        const int v = vb + grp;
-        const bool valid = v < v_end;
-        int s0 = 0, s1 = 0;
-        if (valid) {
-          s1 = __ldg(vend + v);
-          s0 = v > 0 ? __ldg(vend + v - 1) : 0;
-        }
-        T dv;
-        if constexpr (SORTED) {
-          dv = T(sorted_sum(reinterpret_cast<const double*>(u), vsl + s0, s1 - s0, lane));
-        } else {
-          dv = tree_sum<T, G>(u, vsl + s0, s1 - s0, lane);
-        }
-        if (valid && lane == 0) {
-          if (MODE == 1) {
-            dv_out[v] = (double)dv;
-          } else {
-            const T V = cur[v];
-            const int8_t un = unit[v];
-            int kv = kTrials;
-#pragma unroll
-            for (int k = 0; k < kTrials; k++) {
-              const T h = T(0.125 / (double)(1 << k));
-              T c = add(V, mul(h, dv));
-              if (un != 0) c = T(un);
-              c = clampv(c, T(-1), T(1));
-              nxt[(int64_t)k * P.var_cap + v] = c;
-              const bool fail = fabs((double)c - (double)V) >= 1.0;
-              if (!fail && kv == kTrials) kv = k;
-            }
-            kmax = max(kmax, kv);
-          }
-        }
-      }
-      if (MODE == 0) {
-        kmax = warp_max_i(kmax);
-        if ((threadIdx.x & 31) == 0) s_km[threadIdx.x >> 5] = kmax;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          int km = 0;
-          for (int i = 0; i < kThreads / 32; i++) km = max(km, s_km[i]);
-          InstCtrl* S = P.ctrl + s_tile.inst;
-          if (km) atomicMax(&S->acc_kmax, km);
-          __threadfence();
-          const int prev = atomicAdd(&S->vtiles_done, 1);
-          s_last = (prev == I.nvtile - 1);
-        }
-        __syncthreads();
-        if (s_last) {
-          __threadfence();
-          finalize_step<T>(P, I, s_tile.inst, s_red);
-        }
-      }
-    }
-    __syncthreads();
-  }
 }
 
 // ---- setup, state I/O and the reference function-pair mirrors ---------------------------

@@ -103,6 +103,10 @@ class Pack {
   // Enqueues one step as plain launches with CUDA events around each kernel, optionally
   // after writing flush_bytes of scratch (cold L2); accumulates into *t after sync.
   dmm_status profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t);
+  // nsteps steps each launched alone after an L2 flush; summed device time of the steps.
+  dmm_status time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double* ms);
+  // Raises DMM_ERR_CUDA when a cooperative launch reported a grid-barrier timeout.
+  dmm_status check_error();
   dmm_status read_active(int32_t* active);
   // Launches step chunks until no instance is running, or wall_s (> 0) seconds pass, or
   // (stop_after > 0) that many instances finished during the call; keeps one chunk in
@@ -132,6 +136,9 @@ class Pack {
   dmm_status build_csr(const InstDesc& I, const int32_t* lits);
   dmm_status ensure_stage(int64_t doubles);
   dmm_status capture(int32_t steps);
+  dmm_status launch_persist(int32_t nsteps);
+  dmm_status ensure_flush(int64_t bytes);
+  const void* persist_fn() const;
   dmm_status enqueue_step(bool rhs_only, void* dv_out);
   dmm_status enqueue_clause();
   dmm_status enqueue_var(bool rhs_only, void* dv_out);
@@ -185,7 +192,10 @@ class Pack {
   void* flush_ = nullptr;
   int64_t flush_cap_ = 0;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
-  int32_t* pinned_ = nullptr;  // two host-mapped copies of the running-instance count
+  int32_t* pinned_ = nullptr;  // host copies of the running count and finished-ring tail
+  int32_t* live_d_ = nullptr;  // indices of the instances with tiles
+  int32_t* misc_d_ = nullptr;  // [0] live count, [1] barrier error, [2] barrier counter
+  int grid_p_ = 148;           // blocks of the cooperative step kernel
 
   // host mirrors
   std::vector<InstDesc> inst_h_;

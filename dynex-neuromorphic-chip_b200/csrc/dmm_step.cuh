@@ -1,0 +1,477 @@
+// One accepted integration step of the reference integrator (dmm_generate_dxdt and the
+// adaptive dmm_dostep loop, dynex.cc:332-530, 301-327, 1389-1417) as three phases:
+//
+//   A  clause tiles   apply the previous step's deferred Euler update to Xs/Xl (the
+//                     accepted h is only known after every variable is reduced), evaluate
+//                     C_m, G, R and the per-literal contributions u (stored per literal
+//                     slot), count unsatisfied clauses (C_m >= 1/2) and strict-sign
+//                     failures, energy partial per tile.
+//   B  variable tiles reduce each variable's contributions over the variable->slot CSR in
+//                     a fixed order (no atomics), form the four Euler candidates
+//                     V + h dV for h = 1/8 .. 1/64 with unit pin and clamps, and the first
+//                     trial each variable accepts; max over the tile by integer atomic.
+//   F  per instance   accepted trial = max over variables; t += h; solved / step limit.
+//
+// The four candidates replace the reference's retry loop: |clamp(V + h dV) - V| is
+// monotone in h, so the first h the reference accepts is the largest h every variable
+// accepts, i.e. trial max_v k_v; when no trial passes the reference keeps the 1/64 state
+// and advances t by 1/128 (dynex.cc:1401-1411).
+//
+// Two launch forms share the tile code:
+//   k_clause + k_var     one kernel per phase (F runs in the last variable tile of each
+//                        instance); persistent blocks pull tiles from an atomic queue.
+//   k_persist            one cooperative launch runs many steps; each block owns a static
+//                        set of tiles and the phases are separated by grid barriers.
+//
+// Results never depend on the launch form or shape: clause work is per clause,
+// per-variable sums use one canonical order for every lane grouping, tiles never straddle
+// instances, cross-block combinations are integer atomics or fixed-order reductions, and
+// the FP32 energy is summed as exact integers in units of 2^-25.
+#pragma once
+
+#include "dmm_kernels.cuh"
+
+namespace dmm {
+
+constexpr double kEnergyUnitF32 = 33554432.0;  // 2^25: every FP32 C_m is a multiple of 2^-25
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum_d(v);
+  const int w = threadIdx.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = (threadIdx.x < NT / 32) ? red[threadIdx.x] : 0.0;
+    r = warp_sum_d(r);
+  }
+  return r;
+}
+
+struct TileSnap {
+  int32_t done, pending, set, kcur;
+  double h;
+};
+
+template <int NT>
+struct TileSmem {
+  InstDesc inst;
+  TileSnap snap;
+  Tile tile;
+  int cached;  // instance whose description + snapshot are loaded, -1 for none
+  int ti;
+  int flag;
+  double red[NT / 32];
+  int cnt[2][NT / 32];
+};
+
+// Loads tile `ti` and, when its instance differs from the cached one, the instance
+// description and control snapshot.  Block-wide.
+template <class T, int NT>
+__device__ __forceinline__ void load_tile(TileSmem<NT>& sm, const PackView<T>& P, const Tile* tiles,
+                                          int ti) {
+  if (threadIdx.x == 0) {
+    sm.tile = tiles[ti];
+    const int ii = sm.tile.inst;
+    if (ii != sm.cached) {
+      sm.inst = P.inst[ii];
+      const InstCtrl* S = P.ctrl + ii;
+      sm.snap.done = S->done;
+      sm.snap.pending = S->pending;
+      sm.snap.set = S->set;
+      sm.snap.kcur = S->kcur;
+      sm.snap.h = S->h_state;
+      sm.cached = ii;
+    }
+  }
+  __syncthreads();
+}
+
+// ---- phase A -------------------------------------------------------------------------------
+template <class T, bool VEC, int NT>
+__device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
+  if (sm.snap.done != 0) return;  // block-uniform
+  const InstDesc& I = sm.inst;
+  const ClauseConsts<T> kc = make_consts<T>(I, sm.snap.h);
+  const bool pending = sm.snap.pending != 0;
+  const T* __restrict__ V =
+      P.cand + (int64_t)(sm.snap.set * kTrials + sm.snap.kcur) * P.var_cap + I.var0;
+  T* __restrict__ Xs = P.Xs + I.cls0;
+  T* __restrict__ Xl = P.Xl + I.cls0;
+  T* __restrict__ Cp = P.Cp + I.cls0;
+  const T* __restrict__ acm = I.has_alpha_cm ? P.alpha_cm + I.cls0 : nullptr;
+  const int32_t* __restrict__ lit = P.lit + I.slot0;
+  T* __restrict__ u = P.u + I.slot0;
+  const int c_begin = sm.tile.begin, c_end = sm.tile.begin + sm.tile.count;
+  // FP32: energy in exact integer units of 2^-25 (order-independent); FP64: plain sum
+  const double escale = sizeof(T) == 4 ? kEnergyUnitF32 : 1.0;
+  int unsat = 0, vfail = 0;
+  double e = 0.0;
+  auto one_clause = [&](int c) {
+    T xs = Xs[c], xl = Xl[c];
+    const T al = acm ? acm[c] : kc.alpha;
+    if (pending) advance_memory(xs, xl, Cp[c], al, kc);
+    bool ss;
+    T C;
+    if (I.k3) {
+      const int l0 = __ldg(lit + 3 * c), l1 = __ldg(lit + 3 * c + 1), l2 = __ldg(lit + 3 * c + 2);
+      T u0, u1, u2;
+      C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1], xs, xl, kc, u0, u1,
+                  u2, ss);
+      u[3 * c] = u0;
+      u[3 * c + 1] = u1;
+      u[3 * c + 2] = u2;
+    } else {
+      const int s0 = P.coff[I.cls0 + c];
+      const int s1 = (c + 1 < I.m) ? P.coff[I.cls0 + c + 1] : I.nslots;
+      C = clause_general(lit + s0, s1 - s0, V, xs, xl, kc, u + s0, ss);
+    }
+    Xs[c] = xs;
+    Xl[c] = xl;
+    Cp[c] = C;
+    unsat += !(C < T(0.5));
+    vfail += !ss;
+    e += (double)C * escale;
+  };
+  if constexpr (!VEC) {
+    for (int c = c_begin + threadIdx.x; c < c_end; c += NT) one_clause(c);
+  } else if (!I.k3) {
+    for (int c = c_begin + threadIdx.x; c < c_end; c += NT) one_clause(c);
+  } else {
+    // 4 consecutive clauses per thread: 16-byte loads of 12 literals and of Xs, Xl, C;
+    // 16-byte stores of 12 contributions and of Xs, Xl, C.
+    for (int g = c_begin + 4 * threadIdx.x; g < c_end; g += 4 * NT) {
+      if (g + 4 <= c_end) {
+        const int4* L4 = reinterpret_cast<const int4*>(lit + 3 * g);
+        const int4 A = __ldg(L4), B = __ldg(L4 + 1), Cc = __ldg(L4 + 2);
+        const int L[12] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w, Cc.x, Cc.y, Cc.z, Cc.w};
+        const float4 xs4 = *reinterpret_cast<const float4*>(Xs + g);
+        const float4 xl4 = *reinterpret_cast<const float4*>(Xl + g);
+        float4 cp4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (pending) cp4 = *reinterpret_cast<const float4*>(Cp + g);
+        float4 al4 = make_float4(kc.alpha, kc.alpha, kc.alpha, kc.alpha);
+        if (acm) al4 = *reinterpret_cast<const float4*>(acm + g);
+        float xs[4] = {xs4.x, xs4.y, xs4.z, xs4.w};
+        float xl[4] = {xl4.x, xl4.y, xl4.z, xl4.w};
+        const float cp[4] = {cp4.x, cp4.y, cp4.z, cp4.w};
+        const float al[4] = {al4.x, al4.y, al4.z, al4.w};
+        float vv[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) vv[i] = V[abs(L[i]) - 1];
+        float uu[12], cc[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          if (pending) advance_memory(xs[i], xl[i], T(cp[i]), T(al[i]), kc);
+          bool ss;
+          T u0, u1, u2;
+          const T C = clause3(L[3 * i], L[3 * i + 1], L[3 * i + 2], T(vv[3 * i]), T(vv[3 * i + 1]),
+                              T(vv[3 * i + 2]), T(xs[i]), T(xl[i]), kc, u0, u1, u2, ss);
+          uu[3 * i] = u0;
+          uu[3 * i + 1] = u1;
+          uu[3 * i + 2] = u2;
+          cc[i] = C;
+          unsat += !(C < T(0.5));
+          vfail += !ss;
+          e += (double)C * escale;
+        }
+        float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
+        U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
+        U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
+        U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
+        *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
+        *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
+        *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+      } else {
+        for (int c = g; c < c_end; c++) one_clause(c);
+      }
+    }
+  }
+  const int w = threadIdx.x >> 5;
+  unsat = warp_sum_i(unsat);
+  vfail = warp_sum_i(vfail);
+  if ((threadIdx.x & 31) == 0) {
+    sm.cnt[0][w] = unsat;
+    sm.cnt[1][w] = vfail;
+  }
+  const double et = block_sum<NT>(e, sm.red);
+  if (threadIdx.x == 0) {
+    int tu = 0, tv = 0;
+#pragma unroll
+    for (int i = 0; i < NT / 32; i++) {
+      tu += sm.cnt[0][i];
+      tv += sm.cnt[1][i];
+    }
+    InstCtrl* S = P.ctrl + sm.tile.inst;
+    if (tu) atomicAdd(&S->acc_loc, tu);
+    if (tv) atomicAdd(&S->acc_vfail, tv);
+    P.epart[ti] = et;
+  }
+  __syncthreads();
+}
+
+// ---- phase B -------------------------------------------------------------------------------
+// MODE 0: integration step (candidates, trial index).  MODE 1: right-hand side only (dV
+// to dv_out, local variable index).  Returns after a block-wide barrier.
+template <class T, int G, bool SORTED, int MODE, int NT>
+__device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restrict__ dv_out) {
+  if (sm.snap.done != 0) return;  // block-uniform
+  const InstDesc& I = sm.inst;
+  const T* __restrict__ u = P.u + I.slot0;
+  const int32_t* __restrict__ vsl = P.vslot + I.slot0;
+  const int32_t* __restrict__ vend = P.vend + I.var0;
+  const T* __restrict__ cur =
+      P.cand + (int64_t)(sm.snap.set * kTrials + sm.snap.kcur) * P.var_cap + I.var0;
+  T* __restrict__ nxt = P.cand + (int64_t)((sm.snap.set ^ 1) * kTrials) * P.var_cap + I.var0;
+  const int8_t* __restrict__ unit = P.unit + I.var0;
+  constexpr int VPP = NT / G;
+  const int grp = threadIdx.x / G, lane = threadIdx.x % G;
+  const int v_end = sm.tile.begin + sm.tile.count;
+  int kmax = 0;
+  for (int vb = sm.tile.begin; vb < v_end; vb += VPP) {
+    const int v = vb + grp;
+    const bool valid = v < v_end;
+    int s0 = 0, s1 = 0;
+    if (valid) {
+      s1 = __ldg(vend + v);
+      s0 = v > 0 ? __ldg(vend + v - 1) : 0;
+    }
+    T dv;
+    if constexpr (SORTED) {
+      dv = T(sorted_sum(reinterpret_cast<const double*>(u), vsl + s0, s1 - s0, lane));
+    } else {
+      dv = tree_sum<T, G>(u, vsl + s0, s1 - s0, lane);
+    }
+    if (valid && lane == 0) {
+      if (MODE == 1) {
+        dv_out[v] = (double)dv;
+      } else {
+        const T V = cur[v];
+        const int8_t un = unit[v];
+        int kv = kTrials;
+#pragma unroll
+        for (int k = 0; k < kTrials; k++) {
+          const T h = T(0.125 / (double)(1 << k));
+          T c = add(V, mul(h, dv));
+          if (un != 0) c = T(un);
+          c = clampv(c, T(-1), T(1));
+          nxt[(int64_t)k * P.var_cap + v] = c;
+          const bool fail = fabs((double)c - (double)V) >= 1.0;
+          if (!fail && kv == kTrials) kv = k;
+        }
+        kmax = max(kmax, kv);
+      }
+    }
+  }
+  if (MODE == 0) {
+    kmax = warp_max_i(kmax);
+    if ((threadIdx.x & 31) == 0) sm.cnt[0][threadIdx.x >> 5] = kmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int km = 0;
+#pragma unroll
+      for (int i = 0; i < NT / 32; i++) km = max(km, sm.cnt[0][i]);
+      if (km) atomicMax(&P.ctrl[sm.tile.inst].acc_kmax, km);
+    }
+  }
+  __syncthreads();
+}
+
+// ---- phase F -------------------------------------------------------------------------------
+// Finalizes one instance's step (block-wide).  Reads the accumulators of the step, writes
+// the new control state, zeroes the accumulators.
+template <class T, int NT>
+__device__ void finalize_step(const PackView<T>& P, const InstDesc& I, int ii, double* red) {
+  double e = 0.0;
+  for (int i = threadIdx.x; i < I.nctile; i += NT) e = __dadd_rn(e, P.epart[I.ctile0 + i]);
+  e = block_sum<NT>(e, red);
+  if (threadIdx.x == 0) {
+    if (sizeof(T) == 4) e = e * (1.0 / kEnergyUnitF32);
+    InstCtrl* S = P.ctrl + ii;
+    volatile InstCtrl* vS = S;
+    InstCtrl c;
+    // one burst of loads, then one burst of stores
+    c.step = vS->step;
+    c.set = vS->set;
+    c.kcur = vS->kcur;
+    c.best_loc = vS->best_loc;
+    c.t = vS->t;
+    c.best_t = vS->best_t;
+    const int loc = vS->acc_loc;
+    const int vfail = vS->acc_vfail;
+    const int kmax = vS->acc_kmax;
+    const bool solved = (loc == 0 && vfail == 0);
+    const int kacc = kmax < kTrials - 1 ? kmax : kTrials - 1;
+    const double hs = 0.125 / (double)(1 << kacc);
+    const double ht = kmax < kTrials ? hs : 0.0078125;
+    if (loc < c.best_loc) {
+      S->best_loc = loc;
+      S->best_t = c.t;
+    }
+    if (solved) {
+      S->solved_step = c.step;
+      S->solved_t = c.t;
+      S->sol_set = c.set;
+      S->sol_k = c.kcur;
+    }
+    S->loc = loc;
+    S->vfail = vfail;
+    S->energy = e;
+    S->t = __dadd_rn(c.t, ht);
+    S->step = c.step + 1;
+    S->set = c.set ^ 1;
+    S->kcur = kacc;
+    S->h_state = hs;
+    S->pending = 1;
+    S->acc_loc = 0;
+    S->acc_vfail = 0;
+    S->acc_kmax = 0;
+    S->vtiles_done = 0;
+    int st = 0;
+    if (solved) st = 1;
+    else if (I.max_steps > 0 && c.step + 1 >= I.max_steps) st = 2;
+    if (st) {
+      S->done = st;
+      atomicSub(P.active, 1);
+      const int pos = atomicAdd(P.ring_tail, 1);
+      P.ring[pos % P.ring_cap] = ii;
+    }
+    __threadfence();
+  }
+}
+
+// ---- two-kernel form -------------------------------------------------------------------------
+
+template <class T, bool VEC>
+__global__ void __launch_bounds__(kThreads) k_clause(PackView<T> P) {
+  __shared__ TileSmem<kThreads> sm;
+  if (threadIdx.x == 0) {
+    sm.cached = -1;
+    if (blockIdx.x == 0) P.queue[1] = 0;  // the variable-tile queue is idle
+  }
+  const int ntiles = P.ntiles[0];
+  for (;;) {
+    if (threadIdx.x == 0) sm.ti = atomicAdd(&P.queue[0], 1);
+    __syncthreads();
+    const int ti = sm.ti;
+    if (ti >= ntiles) break;
+    load_tile<T, kThreads>(sm, P, P.ctiles, ti);
+    clause_tile<T, VEC, kThreads>(P, sm, ti);
+  }
+}
+
+template <class T, int G, bool SORTED, int MODE>
+__global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restrict__ dv_out) {
+  __shared__ TileSmem<kThreads> sm;
+  if (threadIdx.x == 0) {
+    sm.cached = -1;
+    if (blockIdx.x == 0) P.queue[0] = 0;  // the clause-tile queue is idle
+  }
+  const int ntiles = P.ntiles[1];
+  for (;;) {
+    if (threadIdx.x == 0) sm.ti = atomicAdd(&P.queue[1], 1);
+    __syncthreads();
+    const int ti = sm.ti;
+    if (ti >= ntiles) break;
+    load_tile<T, kThreads>(sm, P, P.vtiles, ti);
+    if (sm.snap.done != 0) continue;
+    var_tile<T, G, SORTED, MODE, kThreads>(P, sm, dv_out);
+    if (MODE == 0) {
+      // the last variable tile of an instance finalizes its step
+      if (threadIdx.x == 0) {
+        __threadfence();
+        const int prev = atomicAdd(&P.ctrl[sm.tile.inst].vtiles_done, 1);
+        sm.flag = (prev == sm.inst.nvtile - 1);
+      }
+      __syncthreads();
+      if (sm.flag) {
+        __threadfence();
+        finalize_step<T, kThreads>(P, sm.inst, sm.tile.inst, sm.red);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---- persistent form -------------------------------------------------------------------------
+
+// Grid barrier for a cooperative launch: a monotonic arrival counter (zeroed before the
+// launch) and a bounded wait.  Returns false, after raising *err, when the wait gives up
+// (the co-residency of a cooperative launch makes this unreachable in practice; the bound
+// keeps a fault from turning into a hang).
+constexpr long long kBarrierSpinLimit = 1ll << 22;  // x ~0.3-1 us per poll: about a second
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <int NT>
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int& target, int* err,
+                                             int* s_ok) {
+  __syncthreads();
+  target += gridDim.x;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    int ok = 1;
+    long long it = 0;
+    while (ld_acquire(bar) < target) {
+      if (++it > kBarrierSpinLimit) {
+        ok = 0;
+        atomicExch(err, 1);
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// nsteps integration steps in one cooperative launch.  Blocks own tiles statically
+// (tile ti -> block ti % gridDim.x); phases A | B | F are separated by grid barriers.
+template <class T, int G, bool SORTED, bool VEC, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_persist(PackView<T> P, int nsteps, unsigned int* bar, int* err) {
+  __shared__ TileSmem<NT> sm;
+  __shared__ int s_ok, s_active;
+  unsigned int target = 0;
+  const int nct = P.ntiles[0], nvt = P.ntiles[1], nlive = *P.nlive;
+  for (int s = 0; s < nsteps; s++) {
+    if (threadIdx.x == 0) {
+      s_active = *(volatile int*)P.active;
+      sm.cached = -1;
+    }
+    __syncthreads();
+    if (s_active <= 0) break;  // grid-uniform: read after a barrier, written before one
+    for (int ti = blockIdx.x; ti < nct; ti += gridDim.x) {
+      load_tile<T, NT>(sm, P, P.ctiles, ti);
+      clause_tile<T, VEC, NT>(P, sm, ti);
+    }
+    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    for (int ti = blockIdx.x; ti < nvt; ti += gridDim.x) {
+      load_tile<T, NT>(sm, P, P.vtiles, ti);
+      var_tile<T, G, SORTED, 0, NT>(P, sm, nullptr);
+    }
+    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    for (int k = blockIdx.x; k < nlive; k += gridDim.x) {
+      if (threadIdx.x == 0) {
+        const int ii = P.live[k];
+        sm.inst = P.inst[ii];
+        sm.flag = (*(volatile int*)&P.ctrl[ii].done == 0);
+        sm.ti = ii;
+      }
+      __syncthreads();
+      if (sm.flag) finalize_step<T, NT>(P, sm.inst, sm.ti, sm.red);
+      __syncthreads();
+    }
+    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+  }
+}
+
+}  // namespace dmm

@@ -5,7 +5,7 @@
 #include <cstdio>
 #include <cstring>
 
-#include "dmm_kernels.cuh"
+#include "dmm_step.cuh"
 #include "dmm_pack.h"
 
 namespace dmm {
@@ -117,8 +117,9 @@ inline int blocks_for(int64_t work, int per = kThreads, int cap = 148 * 16) {
   if (b > cap) b = cap;
   return (int)b;
 }
-constexpr int kClauseTileUnit = 4 * kThreads;  // clauses per pass of the vector path
-constexpr int kVarTileUnit = kThreads;          // variables per tile unit
+constexpr int kMinClauseTile = 256;  // smallest clause tile (bounds the tile tables)
+constexpr int kMinVarTile = 32;      // smallest variable tile
+constexpr int kPersistThreads = 1024;  // block size of the cooperative step kernel
 }  // namespace
 
 int64_t Pack::bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
@@ -128,7 +129,7 @@ int64_t Pack::bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
   m = RangeAlloc::round(std::max<int64_t>(m, 1));
   slots = RangeAlloc::round(std::max<int64_t>(slots, 1));
   int64_t b = m * (3 * t + 4 + (with_alpha_cm ? t : 0)) + slots * (8 + t) + n * (8 * t + 9);
-  b += (m / kClauseTileUnit + 1) * (8 + 16) + (n / kVarTileUnit + 1) * 16;
+  b += (m / kMinClauseTile + 1) * (8 + 16) + (n / kMinVarTile + 1) * 16;
   b += sizeof(InstDesc) + sizeof(InstCtrl) + 8;
   return b;
 }
@@ -142,7 +143,7 @@ Pack::~Pack() {
                   coff_,    lit_,       vslot_,   vend_,       fill_,      unit_,
                   epart_,   inst_d_,    ctrl_d_,  ctiles_d_,   vtiles_d_,  ntiles_d_,
                   queue_d_, active_d_,  ring_d_,  ring_tail_d_, scan_tmp_, longv_d_,
-                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_};
+                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : ev_)
@@ -175,8 +176,8 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   caps_.clauses = RangeAlloc::round(caps_.clauses) + 32 * (int64_t)caps_.insts;
   caps_.slots = RangeAlloc::round(caps_.slots) + 32 * (int64_t)caps_.insts;
   const int64_t V = caps_.vars, C = caps_.clauses, S = caps_.slots, I = caps_.insts;
-  ctile_cap_ = C / kClauseTileUnit + I + 1;
-  vtile_cap_ = V / kVarTileUnit + I + 1;
+  ctile_cap_ = C / kMinClauseTile + I + 1;
+  vtile_cap_ = V / kMinVarTile + I + 1;
   DMM_CUDA(cudaMalloc(&Xs_, C * tsize_));
   DMM_CUDA(cudaMalloc(&Xl_, C * tsize_));
   DMM_CUDA(cudaMalloc(&Cp_, C * tsize_));
@@ -200,6 +201,9 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   DMM_CUDA(cudaMalloc(&ring_d_, I * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&ring_tail_d_, 4 * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&live_d_, I * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&misc_d_, 8 * sizeof(int32_t)));
+  DMM_CUDA(cudaMemsetAsync(misc_d_, 0, 8 * sizeof(int32_t), stream_));
   DMM_CUDA(cudaMemsetAsync(ctrl_d_, 0, I * sizeof(InstCtrl), stream_));
   DMM_CUDA(cudaMemsetAsync(ntiles_d_, 0, 4 * sizeof(int32_t), stream_));
   DMM_CUDA(cudaMemsetAsync(queue_d_, 0, 2 * sizeof(int32_t), stream_));
@@ -219,9 +223,12 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
 
 dmm_status Pack::set_tuning(const dmm_tuning* t) {
   dmm_tuning n = *t;
-  if (n.clause_tile <= 0) n.clause_tile = kClauseTileUnit;
-  if (n.clause_tile % kClauseTileUnit) {
-    set_error("clause_tile must be a multiple of %d", kClauseTileUnit);
+  if (n.clause_tile < 0 || (n.clause_tile > 0 && (n.clause_tile % 4 || n.clause_tile < kMinClauseTile))) {
+    set_error("clause_tile must be 0 (balanced) or a multiple of 4 that is >= %d", kMinClauseTile);
+    return DMM_ERR_ARG;
+  }
+  if (n.var_tile < 0 || (n.var_tile > 0 && n.var_tile < kMinVarTile)) {
+    set_error("var_tile must be 0 (balanced) or >= %d", kMinVarTile);
     return DMM_ERR_ARG;
   }
   if (prec_ == DMM_FP64) {
@@ -231,17 +238,12 @@ dmm_status Pack::set_tuning(const dmm_tuning* t) {
     }
     n.var_group = 32;
   } else {
-    if (n.var_group <= 0) n.var_group = 8;
+    if (n.var_group <= 0) n.var_group = 4;
     if (n.var_group != 1 && n.var_group != 2 && n.var_group != 4 && n.var_group != 8 &&
         n.var_group != 16 && n.var_group != 32) {
       set_error("var_group must be 1, 2, 4, 8, 16 or 32");
       return DMM_ERR_ARG;
     }
-  }
-  if (n.var_tile <= 0) n.var_tile = kVarTileUnit;
-  if (n.var_tile % kVarTileUnit) {
-    set_error("var_tile must be a multiple of %d", kVarTileUnit);
-    return DMM_ERR_ARG;
   }
   if (n.steps_per_graph <= 0) n.steps_per_graph = 32;
   if (n.steps_per_graph > 4096) n.steps_per_graph = 4096;
@@ -249,10 +251,12 @@ dmm_status Pack::set_tuning(const dmm_tuning* t) {
     set_error("blocks_per_sm out of range");
     return DMM_ERR_ARG;
   }
-  const bool retile = n.clause_tile != tun_.clause_tile || n.var_tile != tun_.var_tile;
+  if (n.launch_mode < 0 || n.launch_mode > 1) {
+    set_error("launch_mode must be 0 (cooperative) or 1 (kernel per phase)");
+    return DMM_ERR_ARG;
+  }
   tun_ = n;
   graph_stale_ = true;
-  if (retile && !ctiles_h_.empty()) return commit_tiles();
   if (!ctiles_h_.empty() || !vtiles_h_.empty()) return commit_tiles();
   return DMM_OK;
 }
@@ -626,6 +630,8 @@ void Pack::fill_view(void* vv) const {
   v.ring = ring_d_;
   v.ring_tail = ring_tail_d_;
   v.ring_cap = caps_.insts;
+  v.live = live_d_;
+  v.nlive = misc_d_;
 }
 
 dmm_status Pack::enqueue_clause() {
@@ -681,21 +687,67 @@ dmm_status Pack::enqueue_step(bool rhs_only, void* dv_out) {
   return DMM_OK;
 }
 
-static int occupancy_blocks(const void* fn) {
+static int occupancy_blocks(const void* fn, int threads) {
   int b = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, 0) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, 0) != cudaSuccess) {
     cudaGetLastError();
     b = 4;
   }
   return std::max(1, b);
 }
 
+const void* Pack::persist_fn() const {
+  if (prec_ == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads>;
+  switch (tun_.var_group) {
+    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads>;
+    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads>;
+    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads>;
+    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads>;
+    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads>;
+    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads>;
+  }
+}
+
 dmm_status Pack::commit_tiles() {
   ctiles_h_.clear();
   vtiles_h_.clear();
-  const int TC = tun_.clause_tile, TV = tun_.var_tile;
-  for (int32_t i = 0; i < (int32_t)live_.size(); i++) {
-    if (!live_[i]) continue;
+  std::vector<int32_t> live_list;
+  for (int32_t i = 0; i < (int32_t)live_.size(); i++)
+    if (live_[i]) live_list.push_back(i);
+  // grids
+  int bc, bv;
+  if (prec_ == DMM_FP64) {
+    bc = occupancy_blocks((const void*)k_clause<double, false>, kThreads);
+    bv = occupancy_blocks((const void*)k_var<double, 32, true, 0>, kThreads);
+  } else {
+    bc = occupancy_blocks((const void*)k_clause<float, true>, kThreads);
+    bv = occupancy_blocks((const void*)k_var<float, 8, false, 0>, kThreads);
+  }
+  if (tun_.blocks_per_sm > 0) {
+    bc = std::min(bc, tun_.blocks_per_sm);
+    bv = std::min(bv, tun_.blocks_per_sm);
+  }
+  grid_p_ = occupancy_blocks(persist_fn(), kPersistThreads) * sms_;
+  const bool coop = tun_.launch_mode == 0;
+  const int block = coop ? kPersistThreads : kThreads;
+  const int64_t spread = coop ? grid_p_ : (int64_t)bc * sms_;
+  // tile sizes: balanced over the grid for a single instance, else fixed
+  int TC = tun_.clause_tile, TV = tun_.var_tile;
+  if (TC == 0) {
+    TC = 4 * block;
+    if (live_list.size() == 1) {
+      const int64_t m = inst_h_[live_list[0]].m;
+      TC = (int)std::max<int64_t>(kMinClauseTile, ((m + spread - 1) / spread + 3) & ~int64_t(3));
+    }
+  }
+  if (TV == 0) {
+    TV = block;
+    if (live_list.size() == 1) {
+      const int64_t n = inst_h_[live_list[0]].n;
+      TV = (int)std::max<int64_t>(kMinVarTile, ((n + spread - 1) / spread + 31) & ~int64_t(31));
+    }
+  }
+  for (int32_t i : live_list) {
     InstDesc& I = inst_h_[i];
     I.ctile0 = (int32_t)ctiles_h_.size();
     for (int32_t b = 0; b < I.m; b += TC) ctiles_h_.push_back(Tile{i, b, std::min(TC, I.m - b), 0});
@@ -715,20 +767,13 @@ dmm_status Pack::commit_tiles() {
   if (!vtiles_h_.empty())
     DMM_CUDA(cudaMemcpyAsync(vtiles_d_, vtiles_h_.data(), vtiles_h_.size() * sizeof(Tile),
                              cudaMemcpyHostToDevice, stream_));
+  if (!live_list.empty())
+    DMM_CUDA(cudaMemcpyAsync(live_d_, live_list.data(), live_list.size() * sizeof(int32_t),
+                             cudaMemcpyHostToDevice, stream_));
   int32_t nt[2] = {(int32_t)ctiles_h_.size(), (int32_t)vtiles_h_.size()};
+  int32_t nl = (int32_t)live_list.size();
   DMM_CUDA(cudaMemcpyAsync(ntiles_d_, nt, sizeof nt, cudaMemcpyHostToDevice, stream_));
-  int bc, bv;
-  if (prec_ == DMM_FP64) {
-    bc = occupancy_blocks((const void*)k_clause<double, false>);
-    bv = occupancy_blocks((const void*)k_var<double, 32, true, 0>);
-  } else {
-    bc = occupancy_blocks((const void*)k_clause<float, true>);
-    bv = occupancy_blocks((const void*)k_var<float, 8, false, 0>);
-  }
-  if (tun_.blocks_per_sm > 0) {
-    bc = std::min(bc, tun_.blocks_per_sm);
-    bv = std::min(bv, tun_.blocks_per_sm);
-  }
+  DMM_CUDA(cudaMemcpyAsync(misc_d_, &nl, sizeof nl, cudaMemcpyHostToDevice, stream_));
   const int gc = bc * sms_, gv = bv * sms_;
   const int new_c = fixed_grid_ ? gc : std::max(1, std::min<int>(gc, nt[0]));
   const int new_v = fixed_grid_ ? gv : std::max(1, std::min<int>(gv, nt[1]));
@@ -737,6 +782,37 @@ dmm_status Pack::commit_tiles() {
   grid_v_ = new_v;
   if (!fixed_grid_) graph_stale_ = true;
   DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::launch_persist(int32_t nsteps) {
+  PackView<float> vf;
+  PackView<double> vd;
+  void* view;
+  if (prec_ == DMM_FP64) {
+    fill_view<double>(&vd);
+    view = &vd;
+  } else {
+    fill_view<float>(&vf);
+    view = &vf;
+  }
+  unsigned int* bar = reinterpret_cast<unsigned int*>(misc_d_ + 2);
+  int* err = misc_d_ + 1;
+  DMM_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned int), stream_));
+  void* args[] = {view, &nsteps, &bar, &err};
+  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(kPersistThreads), args, 0,
+                                       stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::check_error() {
+  int32_t e = 0;
+  DMM_CUDA(cudaMemcpyAsync(&e, misc_d_ + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  if (e) {
+    set_error("grid barrier wait gave up in the cooperative step kernel");
+    return DMM_ERR_CUDA;
+  }
   return DMM_OK;
 }
 
@@ -770,6 +846,14 @@ dmm_status Pack::launch_steps(int32_t nsteps) {
   DMM_CUDA(cudaSetDevice(dev_));
   if (ctiles_h_.empty() && vtiles_h_.empty()) return DMM_OK;
   const int32_t S = tun_.steps_per_graph;
+  if (tun_.launch_mode == 0) {
+    while (nsteps > 0) {
+      const int32_t k = std::min(nsteps, S);
+      DMM_TRY(launch_persist(k));
+      nsteps -= k;
+    }
+    return DMM_OK;
+  }
   while (nsteps >= S) {
     if (graph_stale_ || graph_steps_ != S || !graph_exec_) DMM_TRY(capture(S));
     DMM_CUDA(cudaGraphLaunch(graph_exec_, stream_));
@@ -777,6 +861,37 @@ dmm_status Pack::launch_steps(int32_t nsteps) {
   }
   for (int32_t s = 0; s < nsteps; s++) DMM_TRY(enqueue_step(false, nullptr));
   return DMM_OK;
+}
+
+dmm_status Pack::ensure_flush(int64_t flush_bytes) {
+  if (flush_bytes > flush_cap_) {
+    if (flush_) DMM_CUDA(cudaFree(flush_));
+    flush_ = nullptr;
+    DMM_CUDA(cudaMalloc(&flush_, flush_bytes));
+    flush_cap_ = flush_bytes;
+  }
+  return DMM_OK;
+}
+
+dmm_status Pack::time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double* ms) {
+  DMM_CUDA(cudaSetDevice(dev_));
+  DMM_TRY(ensure_flush(flush_bytes));
+  double total = 0.0;
+  for (int32_t s = 0; s < nsteps; s++) {
+    if (flush_bytes > 0) {
+      k_flush<<<sms_ * 4, kThreads, 0, stream_>>>(static_cast<int4*>(flush_), flush_bytes / 16, s);
+      DMM_CUDA(cudaGetLastError());
+    }
+    DMM_CUDA(cudaEventRecord(ev_[0], stream_));
+    DMM_TRY(launch_steps(1));
+    DMM_CUDA(cudaEventRecord(ev_[1], stream_));
+    DMM_CUDA(cudaEventSynchronize(ev_[1]));
+    float a = 0;
+    DMM_CUDA(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+    total += a;
+  }
+  *ms = total;
+  return check_error();
 }
 
 dmm_status Pack::profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t) {
@@ -857,7 +972,7 @@ dmm_status Pack::run(double wall_s, int64_t* steps_launched, bool* timed_out,
     cur = nxt;
   }
   DMM_CUDA(cudaStreamSynchronize(stream_));
-  return DMM_OK;
+  return check_error();
 }
 
 dmm_status Pack::resume(int32_t idx) {
@@ -895,7 +1010,7 @@ dmm_status Pack::stop(int32_t idx, int32_t status) {
 
 dmm_status Pack::sync() {
   DMM_CUDA(cudaStreamSynchronize(stream_));
-  return DMM_OK;
+  return check_error();
 }
 
 dmm_status Pack::rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, double* energy) {

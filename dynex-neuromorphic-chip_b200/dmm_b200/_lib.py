@@ -59,10 +59,10 @@ class Limits(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("clause_tile", ctypes.c_int32), ("var_group", ctypes.c_int32),
                 ("var_tile", ctypes.c_int32), ("steps_per_graph", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("launch_mode", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Cnf(ctypes.Structure):
@@ -124,6 +124,7 @@ SIGNATURES = {
     "dmm_instance_assignment": (_i32, [_vp, _pi8, _pi8]),
     "dmm_instance_profile": (_i32, [_vp, _i32, _i64, _pd, _pd]),
     "dmm_instance_time_steps": (_i32, [_vp, _i32, _pd]),
+    "dmm_instance_time_steps_flushed": (_i32, [_vp, _i32, _i64, _pd]),
     "dmm_batch_create": (_i32, [_i32, _i32, _i32, _i64, _i64, _i64, _P(_vp)]),
     "dmm_batch_destroy": (None, [_vp]),
     "dmm_batch_set_tuning": (_i32, [_vp, _P(Tuning)]),

@@ -172,7 +172,14 @@ class Instance:
         return a.value, b.value
 
     def time_steps(self, nsteps: int) -> float:
-        """Device time (ms) of nsteps steps launched as CUDA-graph chunks."""
+        """Device time (ms) of nsteps steps launched as the solver launches them."""
         ms = ctypes.c_double()
         check(lib().dmm_instance_time_steps(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def time_steps_flushed(self, nsteps: int, flush_bytes: int) -> float:
+        """Summed device time (ms) of nsteps steps, each launched alone after an L2 flush."""
+        ms = ctypes.c_double()
+        check(lib().dmm_instance_time_steps_flushed(self._h, int(nsteps), int(flush_bytes),
+                                                    ctypes.byref(ms)))
         return ms.value

@@ -99,12 +99,14 @@ typedef struct dmm_limits {
 /* Launch shape; 0 in a field selects the default.  Results never depend on it: per-variable
  * sums use a fixed canonical order for every var_group, and tiles never straddle instances. */
 typedef struct dmm_tuning {
-  int32_t clause_tile;      /* clauses per clause tile (multiple of 4*256)                   */
+  int32_t clause_tile;      /* clauses per clause tile (multiple of 4, >= 256; 0: balanced
+                               over the grid for one instance, else 4 x block size)          */
   int32_t var_group;        /* lanes per variable in the dV reduction: 1,2,4,8,16,32         */
-  int32_t var_tile;         /* variables per variable tile                                   */
-  int32_t steps_per_graph;  /* steps captured per CUDA graph launch                          */
-  int32_t blocks_per_sm;    /* persistent blocks per SM for the tile loops                   */
-  int32_t reserved;
+  int32_t var_tile;         /* variables per variable tile (>= 32; 0: as clause_tile)         */
+  int32_t steps_per_graph;  /* steps per launch: per cooperative launch, or per CUDA graph   */
+  int32_t blocks_per_sm;    /* two-kernel form: persistent blocks per SM (0: occupancy)      */
+  int32_t launch_mode;      /* 0: one cooperative launch runs steps_per_graph steps with grid
+                               barriers between phases; 1: one kernel per phase, CUDA graphs */
 } dmm_tuning;
 
 /* A DIMACS formula held in host memory (allocated by the library). */
@@ -209,6 +211,11 @@ dmm_status dmm_instance_profile(dmm_instance* inst, int32_t nsteps, int64_t flus
 /* Benchmark helper: device time (ms) of nsteps steps launched as the solver launches them
  * (CUDA-graph chunks, state resident on the device), one event pair around all of them. */
 dmm_status dmm_instance_time_steps(dmm_instance* inst, int32_t nsteps, double* ms);
+/* Benchmark helper: nsteps steps, each launched on its own (one cooperative launch per
+ * step, or the two phase kernels) after writing flush_bytes of scratch so that it starts
+ * with a cold L2; returns the summed device time of the steps (ms, flushes excluded). */
+dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
+                                           int64_t flush_bytes, double* ms);
 
 /* ---- many formulas in one launch (batched path) -------------------------------------- */
 typedef struct dmm_batch dmm_batch;

@@ -52,16 +52,20 @@ def test_batch_results_equal_alone(fixtures, prec):
 def test_batch_tuning_does_not_change_results(fixtures):
     items = mix(fixtures)
     finals = []
-    for kw in (dict(var_group=1, steps_per_graph=8), dict(var_group=32, steps_per_graph=64,
-                                                           clause_tile=2048, var_tile=512)):
+    for kw in (dict(var_group=1, steps_per_graph=8, launch_mode=0),
+               dict(var_group=32, steps_per_graph=64, clause_tile=2048, var_tile=512,
+                    launch_mode=1),
+               dict(var_group=4, steps_per_graph=5, clause_tile=256, var_tile=32,
+                    launch_mode=0)):
         b = dmm.Batch.for_formulas([f for f, _ in items], precision="fp32")
         b.set_tuning(**kw)
         for form, x0 in items:
             b.add(form, x0, max_steps=120)
         b.run()
         finals.append([b.state(k)[0] for k in range(len(items))])
-    for a, c in zip(*finals):
-        assert np.array_equal(a, c)
+    for other in finals[1:]:
+        for a, c in zip(finals[0], other):
+            assert np.array_equal(a, c)
 
 
 def test_server_results_equal_alone(fixtures):

@@ -144,9 +144,11 @@ def test_fp32_launch_shape_does_not_change_results(fixtures):
     f = fixtures["n1000"]
     x0 = uniform_init(f["n"], f["m"], 41)
     outs = []
-    shapes = [dict(var_group=g, steps_per_graph=s, clause_tile=ct, var_tile=vt)
-              for g, s, ct, vt in [(1, 16, 1024, 256), (2, 7, 2048, 512), (4, 32, 1024, 256),
-                                   (8, 64, 4096, 1024), (16, 3, 1024, 256), (32, 256, 8192, 256)]]
+    shapes = [dict(var_group=g, steps_per_graph=s, clause_tile=ct, var_tile=vt, launch_mode=lm)
+              for g, s, ct, vt, lm in [(1, 16, 1024, 256, 0), (2, 7, 2048, 512, 1),
+                                       (4, 32, 0, 0, 0), (8, 64, 4096, 1024, 1),
+                                       (16, 3, 256, 32, 0), (32, 256, 8192, 256, 1),
+                                       (4, 5, 260, 96, 0)]]
     for kw in shapes:
         with dmm.Instance(formula(f), precision="fp32") as inst:
             inst.set_tuning(**kw)
