@@ -130,7 +130,7 @@ __device__ __forceinline__ T clause3(int l0, int l1, int l2, T v0, T v1, T v2, T
 // the same values as this loop; k = 1 runs no branch, C = 0; k = 0 leaves C = INT_MAX/2).
 template <class T>
 __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int k,
-                                            const T* __restrict__ V, T Xs, T Xl,
+                                            const T* V, T Xs, T Xl,
                                             const ClauseConsts<T>& kc, T* __restrict__ u,
                                             bool& strict_sat) {
   const T one = T(1), half = T(0.5), zero = T(0);
@@ -184,7 +184,7 @@ __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int
 // holds virtual lanes lane + G*i; butterflies with offset >= G are lane-local, smaller
 // ones are shuffles.  Every G gives the same value.  All 32 lanes of the warp must call.
 template <class T, int G>
-__device__ __forceinline__ T tree_sum(const T* __restrict__ u, const int32_t* __restrict__ vs,
+__device__ __forceinline__ T tree_sum(const T* u, const int32_t* __restrict__ vs,
                                       int d, int lane) {
   constexpr int NV = 32 / G;
   T p[NV];
@@ -214,7 +214,7 @@ __device__ __forceinline__ T tree_sum(const T* __restrict__ u, const int32_t* __
 // right from +0.0 (zero contributions, which the reference skips, change no partial sum).
 // One warp per variable; d must be warp-uniform.  Bitonic sort in registers for d <= 32R.
 template <int R>
-__device__ __forceinline__ double sorted_sum_reg(const double* __restrict__ u,
+__device__ __forceinline__ double sorted_sum_reg(const double* u,
                                                  const int32_t* __restrict__ vs, int d,
                                                  int lane) {
   double a[R];
@@ -271,7 +271,7 @@ __device__ __forceinline__ double sorted_sum_reg(const double* __restrict__ u,
 
 // Long lists: repeated selection of the next (value, position) pair in lexicographic
 // order; O(d^2 / 32) loads, no scratch memory.
-__device__ __noinline__ double sorted_sum_select(const double* __restrict__ u,
+__device__ __noinline__ double sorted_sum_select(const double* u,
                                                  const int32_t* __restrict__ vs, int d,
                                                  int lane) {
   double acc = 0.0;
@@ -305,7 +305,7 @@ __device__ __noinline__ double sorted_sum_select(const double* __restrict__ u,
   return acc;
 }
 
-__device__ __forceinline__ double sorted_sum(const double* __restrict__ u,
+__device__ __forceinline__ double sorted_sum(const double* u,
                                              const int32_t* __restrict__ vs, int d, int lane) {
   if (d <= 32) return sorted_sum_reg<1>(u, vs, d, lane);
   if (d <= 64) return sorted_sum_reg<2>(u, vs, d, lane);

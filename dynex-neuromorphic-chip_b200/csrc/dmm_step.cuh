@@ -96,7 +96,7 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
   const InstDesc& I = sm.inst;
   const ClauseConsts<T> kc = make_consts<T>(I, sm.snap.h);
   const bool pending = sm.snap.pending != 0;
-  const T* __restrict__ V =
+  const T* V =
       P.cand + (int64_t)(sm.snap.set * kTrials + sm.snap.kcur) * P.var_cap + I.var0;
   T* __restrict__ Xs = P.Xs + I.cls0;
   T* __restrict__ Xl = P.Xl + I.cls0;
@@ -218,10 +218,10 @@ template <class T, int G, bool SORTED, int MODE, int NT>
 __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restrict__ dv_out) {
   if (sm.snap.done != 0) return;  // block-uniform
   const InstDesc& I = sm.inst;
-  const T* __restrict__ u = P.u + I.slot0;
+  const T* u = P.u + I.slot0;
   const int32_t* __restrict__ vsl = P.vslot + I.slot0;
   const int32_t* __restrict__ vend = P.vend + I.var0;
-  const T* __restrict__ cur =
+  const T* cur =
       P.cand + (int64_t)(sm.snap.set * kTrials + sm.snap.kcur) * P.var_cap + I.var0;
   T* __restrict__ nxt = P.cand + (int64_t)((sm.snap.set ^ 1) * kTrials) * P.var_cap + I.var0;
   const int8_t* __restrict__ unit = P.unit + I.var0;
