@@ -1020,10 +1020,10 @@ dmm_status Pack::rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, d
   const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
   // tiles of this instance only
   std::vector<Tile> ct, vt;
-  for (int32_t b = 0; b < I.m; b += tun_.clause_tile)
-    ct.push_back(Tile{idx, b, std::min(tun_.clause_tile, I.m - b), 0});
-  for (int32_t b = 0; b < I.n; b += tun_.var_tile)
-    vt.push_back(Tile{idx, b, std::min(tun_.var_tile, I.n - b), 0});
+  // the right-hand side runs the kernel-per-phase form with its own fixed tiles
+  const int TC = 4 * kThreads, TV = kThreads;
+  for (int32_t b = 0; b < I.m; b += TC) ct.push_back(Tile{idx, b, std::min(TC, I.m - b), 0});
+  for (int32_t b = 0; b < I.n; b += TV) vt.push_back(Tile{idx, b, std::min(TV, I.n - b), 0});
   const int64_t need = std::max<int64_t>(std::max(ct.size(), vt.size()), 1);
   if (need > aux_cap_) {
     if (aux_ctiles_d_) DMM_CUDA(cudaFree(aux_ctiles_d_));
