@@ -25,8 +25,8 @@ OBJ_DIR = os.path.join(HERE, "lib", "obj")
 LIB = os.path.join(LIB_DIR, "libdmm.so")
 CLI = os.path.join(BIN_DIR, "dynex")
 
-SOURCES = ["pack.cu", "cnf.cpp", "capi.cpp", "server.cpp"]
-HEADERS = ["dmm_device.cuh", "dmm_kernels.cuh", "dmm_pack.h"]
+SOURCES = ["pack.cu", "cnf.cpp", "capi.cpp", "server.cpp", "noalloc.cu"]
+HEADERS = ["dmm_device.cuh", "dmm_kernels.cuh", "dmm_step.cuh", "dmm_pack.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -271,7 +271,7 @@ __device__ __forceinline__ double sorted_sum_reg(const double* u,
 
 // Long lists: repeated selection of the next (value, position) pair in lexicographic
 // order; O(d^2 / 32) loads, no scratch memory.
-__device__ __noinline__ double sorted_sum_select(const double* u,
+static __device__ __noinline__ double sorted_sum_select(const double* u,
                                                  const int32_t* __restrict__ vs, int d,
                                                  int lane) {
   double acc = 0.0;
@@ -317,13 +317,13 @@ __device__ __forceinline__ double sorted_sum(const double* u,
 // ---- setup, state I/O and the reference function-pair mirrors ---------------------------
 
 // Occurrence count of every variable (the reference's numOccurrenceT, dynex.cc:2380-2383).
-__global__ void k_count(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ deg) {
+static __global__ void k_count(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ deg) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x)
     atomicAdd(&deg[abs(lit[s]) - 1], 1);
 }
 
 // Inclusive scan, 2048 elements per block; block totals to `sums`.
-__global__ void k_scan_block(int32_t* __restrict__ a, int len, int32_t* __restrict__ sums) {
+static __global__ void k_scan_block(int32_t* __restrict__ a, int len, int32_t* __restrict__ sums) {
   constexpr int IPT = 8;
   __shared__ int32_t s[kThreads];
   const int base = blockIdx.x * kThreads * IPT + threadIdx.x * IPT;
@@ -350,7 +350,7 @@ __global__ void k_scan_block(int32_t* __restrict__ a, int len, int32_t* __restri
   if (threadIdx.x == kThreads - 1 && sums) sums[blockIdx.x] = s[kThreads - 1];
 }
 
-__global__ void k_scan_add(int32_t* __restrict__ a, int len, const int32_t* __restrict__ sums) {
+static __global__ void k_scan_add(int32_t* __restrict__ a, int len, const int32_t* __restrict__ sums) {
   constexpr int IPT = 8;
   if (blockIdx.x == 0) return;
   const int32_t add_v = sums[blockIdx.x - 1];
@@ -360,12 +360,12 @@ __global__ void k_scan_add(int32_t* __restrict__ a, int len, const int32_t* __re
     if (base + i < len) a[base + i] += add_v;
 }
 
-__global__ void k_fill_start(const int32_t* __restrict__ vend, int n, int32_t* __restrict__ fill) {
+static __global__ void k_fill_start(const int32_t* __restrict__ vend, int n, int32_t* __restrict__ fill) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
     fill[v] = v > 0 ? vend[v - 1] : 0;
 }
 
-__global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ fill,
+static __global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ fill,
                           int32_t* __restrict__ vslot) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
     const int pos = atomicAdd(&fill[abs(lit[s]) - 1], 1);
@@ -377,7 +377,7 @@ __global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, int32_t* 
 // memory) so the CSR is independent of the scatter's atomic order.  Lists longer than
 // kSortCap are reported in `longv` for the host.
 constexpr int kSortCap = 1024;
-__global__ void __launch_bounds__(kThreads) k_sort_lists(const int32_t* __restrict__ vend, int n,
+static __global__ void __launch_bounds__(kThreads) k_sort_lists(const int32_t* __restrict__ vend, int n,
                                                          int32_t* __restrict__ vslot,
                                                          int32_t* __restrict__ longv,
                                                          int32_t* __restrict__ nlong) {
@@ -503,7 +503,7 @@ __global__ void k_dostep(const InstDesc* __restrict__ insts, int ii, const int8_
 
 // Sum of an instance's energy partials and its loc/strict counters after a right-hand-side
 // evaluation; zeroes the accumulators.  One block.
-__global__ void k_rhs_finish(const InstDesc* __restrict__ insts, InstCtrl* __restrict__ ctrl, int ii,
+static __global__ void k_rhs_finish(const InstDesc* __restrict__ insts, InstCtrl* __restrict__ ctrl, int ii,
                              const double* __restrict__ epart) {
   __shared__ double red[kThreads / 32];
   const InstDesc I = insts[ii];
@@ -523,7 +523,7 @@ __global__ void k_rhs_finish(const InstDesc* __restrict__ insts, InstCtrl* __res
 }
 
 // Writes a large buffer so that the next kernel starts with a cold L2 (benchmarks).
-__global__ void k_flush(int4* __restrict__ buf, int64_t n16, int salt) {
+static __global__ void k_flush(int4* __restrict__ buf, int64_t n16, int salt) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16;
        i += (int64_t)gridDim.x * blockDim.x)
     buf[i] = make_int4(salt, (int)i, salt, (int)i);
