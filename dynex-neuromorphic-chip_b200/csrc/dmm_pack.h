@@ -137,6 +137,7 @@ class Pack {
   dmm_status ensure_stage(int64_t doubles);
   dmm_status capture(int32_t steps);
   dmm_status launch_persist(int32_t nsteps);
+  dmm_status launch_inst(int32_t nsteps);
   dmm_status ensure_flush(int64_t bytes);
   const void* persist_fn() const;
   dmm_status enqueue_step(bool rhs_only, void* dv_out);
@@ -194,7 +195,10 @@ class Pack {
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* pinned_ = nullptr;  // host copies of the running count and finished-ring tail
   int32_t* live_d_ = nullptr;  // indices of the instances with tiles
-  int32_t* misc_d_ = nullptr;  // [0] live count, [1] barrier error, [2] barrier counter
+  int32_t* misc_d_ = nullptr;  // [0] live count, [1] barrier error, [2] barrier counter,
+                               // [3] formula queue of the one-block-per-formula kernel
+  int32_t* order_d_ = nullptr; // formulas run one block each, largest first
+  int32_t n_small_ = 0;
   int grid_p_ = 148;           // blocks of the cooperative step kernel
 
   // host mirrors

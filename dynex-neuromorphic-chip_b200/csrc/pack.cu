@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "dmm_inst.cuh"
 #include "dmm_step.cuh"
 #include "dmm_pack.h"
 
@@ -143,7 +144,7 @@ Pack::~Pack() {
                   coff_,    lit_,       vslot_,   vend_,       fill_,      unit_,
                   epart_,   inst_d_,    ctrl_d_,  ctiles_d_,   vtiles_d_,  ntiles_d_,
                   queue_d_, active_d_,  ring_d_,  ring_tail_d_, scan_tmp_, longv_d_,
-                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_};
+                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_, order_d_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : ev_)
@@ -202,6 +203,7 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   DMM_CUDA(cudaMalloc(&ring_tail_d_, 4 * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&live_d_, I * sizeof(int32_t)));
+  DMM_CUDA(cudaMalloc(&order_d_, I * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&misc_d_, 8 * sizeof(int32_t)));
   DMM_CUDA(cudaMemsetAsync(misc_d_, 0, 8 * sizeof(int32_t), stream_));
   DMM_CUDA(cudaMemsetAsync(ctrl_d_, 0, I * sizeof(InstCtrl), stream_));
@@ -251,8 +253,9 @@ dmm_status Pack::set_tuning(const dmm_tuning* t) {
     set_error("blocks_per_sm out of range");
     return DMM_ERR_ARG;
   }
-  if (n.launch_mode < 0 || n.launch_mode > 1) {
-    set_error("launch_mode must be 0 (cooperative) or 1 (kernel per phase)");
+  if (n.launch_mode < 0 || n.launch_mode > 3) {
+    set_error("launch_mode must be 0 (auto), 1 (kernel per phase), 2 (cooperative tiles) or "
+              "3 (one block per small formula)");
     return DMM_ERR_ARG;
   }
   tun_ = n;
@@ -712,8 +715,36 @@ dmm_status Pack::commit_tiles() {
   ctiles_h_.clear();
   vtiles_h_.clear();
   std::vector<int32_t> live_list;
-  for (int32_t i = 0; i < (int32_t)live_.size(); i++)
-    if (live_[i]) live_list.push_back(i);
+  // formulas that one block integrates alone (FP32, V and dV fit in shared memory): used
+  // when there are enough of them to fill the GPU (auto) or when forced (launch_mode 3)
+  std::vector<int32_t> small_list;
+  {
+    std::vector<int32_t> eligible, others;
+    for (int32_t i = 0; i < (int32_t)live_.size(); i++) {
+      if (!live_[i]) continue;
+      const bool ok = prec_ == DMM_FP32 && inst_h_[i].n <= kInstVCap &&
+                      (tun_.launch_mode == 0 || tun_.launch_mode == 3);
+      (ok ? eligible : others).push_back(i);
+    }
+    const bool use_small = tun_.launch_mode == 3 || (int64_t)eligible.size() >= sms_;
+    if (use_small) {
+      small_list = eligible;
+    } else {
+      others.insert(others.end(), eligible.begin(), eligible.end());
+      std::sort(others.begin(), others.end());
+    }
+    live_list = others;
+    std::stable_sort(small_list.begin(), small_list.end(),
+                     [&](int32_t a, int32_t b) { return inst_h_[a].m > inst_h_[b].m; });
+  }
+  for (int32_t i : small_list) {
+    inst_h_[i].ctile0 = inst_h_[i].nctile = inst_h_[i].vtile0 = inst_h_[i].nvtile = 0;
+    DMM_TRY(upload_desc(i));
+  }
+  if (!small_list.empty())
+    DMM_CUDA(cudaMemcpyAsync(order_d_, small_list.data(), small_list.size() * sizeof(int32_t),
+                             cudaMemcpyHostToDevice, stream_));
+  n_small_ = (int32_t)small_list.size();
   // grids
   int bc, bv;
   if (prec_ == DMM_FP64) {
@@ -728,7 +759,7 @@ dmm_status Pack::commit_tiles() {
     bv = std::min(bv, tun_.blocks_per_sm);
   }
   grid_p_ = occupancy_blocks(persist_fn(), kPersistThreads) * sms_;
-  const bool coop = tun_.launch_mode == 0;
+  const bool coop = tun_.launch_mode != 1;
   const int block = coop ? kPersistThreads : kThreads;
   const int64_t spread = coop ? grid_p_ : (int64_t)bc * sms_;
   // tile sizes: balanced over the grid for a single instance, else fixed
@@ -805,6 +836,36 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
   return DMM_OK;
 }
 
+template <int G>
+static dmm_status launch_inst_g(const PackView<float>& v, const int32_t* order, int count,
+                                int nsteps, int* queue, int grid, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    DMM_CUDA(cudaFuncSetAttribute(k_inst<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kInstSmem));
+    attr = true;
+  }
+  k_inst<G><<<grid, kInstThreads, kInstSmem, s>>>(v, order, count, nsteps, queue);
+  DMM_CUDA(cudaGetLastError());
+  return DMM_OK;
+}
+
+dmm_status Pack::launch_inst(int32_t nsteps) {
+  PackView<float> v;
+  fill_view<float>(&v);
+  int* queue = misc_d_ + 3;
+  DMM_CUDA(cudaMemsetAsync(queue, 0, sizeof(int32_t), stream_));
+  const int grid = std::max(1, std::min(sms_, (int)n_small_));
+  switch (tun_.var_group) {
+    case 1: return launch_inst_g<1>(v, order_d_, n_small_, nsteps, queue, grid, stream_);
+    case 2: return launch_inst_g<2>(v, order_d_, n_small_, nsteps, queue, grid, stream_);
+    case 4: return launch_inst_g<4>(v, order_d_, n_small_, nsteps, queue, grid, stream_);
+    case 8: return launch_inst_g<8>(v, order_d_, n_small_, nsteps, queue, grid, stream_);
+    case 16: return launch_inst_g<16>(v, order_d_, n_small_, nsteps, queue, grid, stream_);
+    default: return launch_inst_g<32>(v, order_d_, n_small_, nsteps, queue, grid, stream_);
+  }
+}
+
 dmm_status Pack::check_error() {
   int32_t e = 0;
   DMM_CUDA(cudaMemcpyAsync(&e, misc_d_ + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
@@ -844,12 +905,13 @@ dmm_status Pack::capture(int32_t steps) {
 
 dmm_status Pack::launch_steps(int32_t nsteps) {
   DMM_CUDA(cudaSetDevice(dev_));
-  if (ctiles_h_.empty() && vtiles_h_.empty()) return DMM_OK;
+  if (ctiles_h_.empty() && vtiles_h_.empty() && n_small_ == 0) return DMM_OK;
   const int32_t S = tun_.steps_per_graph;
-  if (tun_.launch_mode == 0) {
+  if (tun_.launch_mode != 1) {
     while (nsteps > 0) {
       const int32_t k = std::min(nsteps, S);
-      DMM_TRY(launch_persist(k));
+      if (!ctiles_h_.empty() || !vtiles_h_.empty()) DMM_TRY(launch_persist(k));
+      if (n_small_ > 0) DMM_TRY(launch_inst(k));
       nsteps -= k;
     }
     return DMM_OK;

@@ -32,9 +32,13 @@ def mix(fixtures):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
-def test_batch_results_equal_alone(fixtures, prec):
+@pytest.mark.parametrize("mode", [0, 3])
+def test_batch_results_equal_alone(fixtures, prec, mode):
+    if prec == "fp64" and mode == 3:
+        pytest.skip("one block per formula is the FP32 production path")
     items = mix(fixtures)
     b = dmm.Batch.for_formulas([f for f, _ in items], precision=prec)
+    b.set_tuning(launch_mode=mode)
     for form, x0 in items:
         b.add(form, x0, max_steps=300)
     stats = b.run()
@@ -56,7 +60,9 @@ def test_batch_tuning_does_not_change_results(fixtures):
                dict(var_group=32, steps_per_graph=64, clause_tile=2048, var_tile=512,
                     launch_mode=1),
                dict(var_group=4, steps_per_graph=5, clause_tile=256, var_tile=32,
-                    launch_mode=0)):
+                    launch_mode=2),
+               dict(var_group=8, steps_per_graph=7, launch_mode=3),
+               dict(var_group=2, steps_per_graph=300, launch_mode=3)):
         b = dmm.Batch.for_formulas([f for f, _ in items], precision="fp32")
         b.set_tuning(**kw)
         for form, x0 in items:
@@ -158,3 +164,24 @@ def test_full_size_fp32_properties(big):
     a = (np.float32(1) - q * v[np.abs(lits) - 1]).min(axis=1) * np.float32(0.5)
     assert loc == int((a >= 0.5).sum())
     assert dmm.check_assignment(form, planted) == 0
+
+
+def test_many_small_formulas_auto_mode_equal_alone(fixtures):
+    """More small formulas than SMs: the automatic launch runs one block per formula; every
+    formula's result equals its run alone."""
+    f = fixtures["n100"]
+    form = formula(f)
+    count = 300
+    x0s = [uniform_init(f["n"], f["m"], 500 + k) for k in range(count)]
+    b = dmm.Batch(count, count * f["n"], count * f["m"], count * 3 * f["m"], precision="fp32")
+    for x0 in x0s:
+        b.add(form, x0, max_steps=400)
+    stats = b.run()
+    assert stats["solved"] + stats["unsolved"] == count
+    for k in (0, 1, 77, 150, 299):
+        r_b, post_b = b.result(k)
+        r_a, post_a, x_a = alone(form, x0s[k], "fp32", 400)
+        assert (r_b.status, r_b.steps, r_b.solved_step, r_b.t, r_b.loc) == (
+            r_a.status, r_a.steps, r_a.solved_step, r_a.t, r_a.loc)
+        assert np.array_equal(b.state(k)[0], x_a)
+        assert np.array_equal(post_b, post_a)

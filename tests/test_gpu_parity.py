@@ -148,7 +148,7 @@ def test_fp32_launch_shape_does_not_change_results(fixtures):
               for g, s, ct, vt, lm in [(1, 16, 1024, 256, 0), (2, 7, 2048, 512, 1),
                                        (4, 32, 0, 0, 0), (8, 64, 4096, 1024, 1),
                                        (16, 3, 256, 32, 0), (32, 256, 8192, 256, 1),
-                                       (4, 5, 260, 96, 0)]]
+                                       (4, 5, 260, 96, 2), (8, 9, 0, 0, 3), (1, 40, 0, 0, 3)]]
     for kw in shapes:
         with dmm.Instance(formula(f), precision="fp32") as inst:
             inst.set_tuning(**kw)
