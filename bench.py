@@ -53,7 +53,58 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and served workloads (rank 0, one GPU)")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="only run the FP32-vs-FP64 study (n=1,000,000) and print its line")
+    ap.add_argument("--study-n", type=int, default=1_000_000)
+    ap.add_argument("--study-seeds", type=int, default=16)
     return ap.parse_args()
+
+
+def run_extras(device: int) -> dict:
+    """The batched and served configurations (see dmm_b200/workloads.py), each against the
+    plain path that takes the same formulas one at a time.  Per-formula results are
+    identical on every path, so the solve rates are equal by construction."""
+    import numpy as np
+
+    from dmm_b200 import workloads as w
+
+    items = w.make_items(4096, 100, 5000, ratios=(8.0,), seed=1)
+    b = w.run_batched(items, max_steps=2000, device=device)
+    sample = items[:64]
+    p = w.run_plain(sample, max_steps=2000, device=device)
+    pb = w.run_batched(sample, max_steps=2000, device=device)
+    assert p["steps"] == pb["steps"], "per-formula results differ between paths"
+    batched = {
+        "workload": "4096 planted 3-SAT formulas, n log-uniform [100, 5000], r=8, p0=0.08, "
+                    "FP32, step cap 2000, one pack",
+        "clause_updates_per_s": b["clause_updates_per_s"], "device_ms": b["device_ms"],
+        "solved": b["solved"], "instances": b["instances"],
+        "solves_per_s": b["solves_per_s_run"], "solves_per_s_incl_setup": b["solves_per_s"],
+        "setup_s": b["setup_s"],
+        "steps_p50_p99_max": [float(x) for x in np.percentile(b["steps"], [50, 99, 100])],
+        "plain_sample": {"instances": p["instances"], "solved": p["solved"],
+                         "solves_per_s": p["solves_per_s"],
+                         "clause_updates_per_s": p["clause_updates_per_s"],
+                         "path": "dmm_instance create + solve, one formula at a time"},
+        "batched_same_sample_solves_per_s": pb["solves_per_s_run"],
+        "solves_ratio_vs_plain": b["solves_per_s_run"] / max(p["solves_per_s"], 1e-9),
+    }
+    sv = w.make_items(300, 100, 100000, ratios=(4.3, 6.0, 8.0), seed=2)
+    arr = w.poisson_times(len(sv), 200.0, seed=2)
+    s = w.run_served(sv, arr, budget_bytes=150 << 30, max_steps=3000, device=device)
+    sp = w.run_served_plain(sv, arr, max_steps=3000, device=device)
+    served = {
+        "workload": "300 requests, Poisson 200/s, planted 3-SAT n log-uniform [100, 100000], "
+                    "r in {4.3, 6, 8}, p0=0.08, FP32, step cap 3000, budget 150 GB",
+        "solved": s["solved"], "requests": s["requests"], "solves_per_s": s["solves_per_s"],
+        "p50_tts_s": s["p50_tts_s"], "p99_tts_s": s["p99_tts_s"], "wall_s": s["wall_s"],
+        "plain": {"solved": sp["solved"], "solves_per_s": sp["solves_per_s"],
+                  "p50_tts_s": sp["p50_tts_s"], "p99_tts_s": sp["p99_tts_s"],
+                  "path": "same arrivals, one request at a time"},
+    }
+    return {"batched": batched, "served": served}
 
 
 # ---- helpers ------------------------------------------------------------------------------
@@ -200,6 +251,13 @@ def main():
     if a.impl == "reference":
         run_reference_arm(a)
         return
+    if a.precision_study:
+        from dmm_b200 import workloads as w
+
+        r = w.precision_study(n=a.study_n, seeds=range(a.study_seeds))
+        print(json.dumps({"precision_study": r, "workload": f"planted 3-SAT n={a.study_n}, "
+                          "r=8, p0=0.08, FP32 vs FP64 from the same initial states"}), flush=True)
+        return
     import numpy as np
     import torch
 
@@ -312,6 +370,10 @@ def main():
                "sample": f"{CPU_SAMPLE_STEPS} steps of the same instance and initial state, "
                          "reference dynex.cc right-hand side + Euler step, 1 thread"}
 
+    extras = None
+    if rank == 0 and world == 1 and not a.no_extras:
+        extras = run_extras(local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "clause-updates/s", "n_gpus": world,
@@ -338,6 +400,8 @@ def main():
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if extras is not None:
+            line.update(extras)
         print(json.dumps(line), flush=True)
     inst.close()
     if dist is not None:

@@ -94,6 +94,55 @@ def run_plain(items: list[Item], max_steps: int, device: int = 0) -> dict:
             "clause_updates_per_s": updates / dt, "steps": steps, "solved_flags": flags}
 
 
+def precision_study(n: int = 1_000_000, r: float = 8.0, seeds=range(8),
+                    checkpoints=(10, 100, 1000), max_steps: int = 5000, instance_seed: int = 7,
+                    device: int = 0) -> dict:
+    """FP32 production path against the FP64 path (the reference's arithmetic) on one planted
+    formula from several initial states: max |dV| and |dXl| at each checkpoint step (while
+    both runs are still integrating), then solve rate and steps-to-solution of each."""
+    f, _ = generate_planted(n, int(round(r * n)), 0.08, 0.46, seed=instance_seed)
+    errs = {c: {"dv": [], "dxl": []} for c in checkpoints}
+    res = {"fp32": [], "fp64": []}
+    i32 = Instance(f, precision="fp32", device=device)
+    i64 = Instance(f, precision="fp64", device=device)
+    try:
+        for s in seeds:
+            x0 = initial_state_uniform(f, 10_000 + s)
+            i32.set_state(x0)
+            i64.set_state(x0)
+            done = 0
+            for c in checkpoints:
+                a = i32.step(c - done)
+                b = i64.step(c - done)
+                done = c
+                if a.status != 0 or b.status != 0:
+                    break
+                xa, _ = i32.get_state()
+                xb, _ = i64.get_state()
+                errs[c]["dv"].append(float(np.max(np.abs(xa[:n] - xb[:n]))))
+                errs[c]["dxl"].append(float(np.max(np.abs(xa[n + f.m:] - xb[n + f.m:]))))
+            for name, inst in (("fp32", i32), ("fp64", i64)):
+                rr = inst.solve(max_steps=max_steps)
+                res[name].append((rr.solved, rr.solved_step if rr.solved else rr.steps))
+    finally:
+        i32.close()
+        i64.close()
+    out = {"n": n, "m": f.m, "seeds": len(list(seeds)), "max_steps": max_steps, "checkpoints": {}}
+    for c in checkpoints:
+        if errs[c]["dv"]:
+            out["checkpoints"][str(c)] = {"runs": len(errs[c]["dv"]),
+                                          "max_abs_dv": max(errs[c]["dv"]),
+                                          "max_abs_dxl": max(errs[c]["dxl"]),
+                                          "median_max_abs_dv": float(np.median(errs[c]["dv"]))}
+    for name in ("fp32", "fp64"):
+        solved = [st for ok, st in res[name] if ok]
+        out[name] = {"solve_rate": len(solved) / max(1, len(res[name])),
+                     "steps_p50": float(np.median(solved)) if solved else None,
+                     "steps_p90": float(np.percentile(solved, 90)) if solved else None,
+                     "steps": [st for _, st in res[name]]}
+    return out
+
+
 def poisson_times(count: int, rate: float, seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed + 99)
     return np.cumsum(rng.exponential(1.0 / rate, size=count))

@@ -1,0 +1,79 @@
+"""The drop-in command line: `dynex -i file.cnf` on the GPU reproduces the reference CLI's
+known answers (step count, T, reported assignment) and its report and solution file."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import dmm_b200 as dmm
+from dmm_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def run_cli(args, timeout=300):
+    r = subprocess.run([_lib.CLI_PATH] + args, capture_output=True, text=True, timeout=timeout)
+    assert r.returncode == 0, r.stderr
+    return r.stdout
+
+
+def parse(out):
+    m = re.search(r"c \[(\d+)\] T=([0-9.]+) SOLUTION FOUND", out)
+    steps = int(re.search(r"STEPS = (\d+)", out).group(1))
+    v = []
+    for line in out.splitlines():
+        if line.startswith("v "):
+            v += [int(t) for t in line[2:].split()]
+    assert v and v[-1] == 0
+    return {"T": float(m.group(2)) if m else None, "steps": steps, "v": v[:-1],
+            "verified": "SAT (VERIFIED)" in out, "sat": "SATISFIABLE" in out}
+
+
+@pytest.mark.parametrize("name,seed", [("n100", 0), ("n200", 1), ("n500", 2), ("n1000", 0)])
+def test_cli_matches_reference_known_answers(tmp_path, fixtures, known_answers, name, seed):
+    f = fixtures[name]
+    path = str(tmp_path / f"{name}.cnf")
+    dmm.write_cnf(dmm.from_arrays(f["lits"], f["off"], f["n"]), path)
+    out = parse(run_cli(["-i", path, "-l", str(seed)]))
+    ka = known_answers["cli"][f"{name}_seed{seed}"]
+    assert out["sat"] and out["verified"]
+    assert out["steps"] == ka["steps"]
+    assert out["T"] == pytest.approx(ka["T"], abs=1e-9)
+    assert out["v"] == ka["v"]
+    # the solution file in the reference's format (dynex.cc:693-699)
+    sol = open(path + ".solution.txt").read().split(",")
+    lits = [int(t) for t in sol if t.strip()]
+    assert len(lits) == f["n"]
+    assign = np.array([1 if l > 0 else -1 for l in lits], np.int8)
+    assert dmm.check_assignment(dmm.from_arrays(f["lits"], f["off"], f["n"]), assign) == 0
+
+
+def test_cli_replicas_and_fp32(tmp_path, fixtures):
+    f = fixtures["n500"]
+    form = dmm.from_arrays(f["lits"], f["off"], f["n"])
+    path = str(tmp_path / "n500.cnf")
+    dmm.write_cnf(form, path)
+    for args in (["-w", "3", "-l", "0"], ["-P", "fp32", "-l", "4"], ["-w", "4", "-P", "fp32"]):
+        out = parse(run_cli(["-i", path] + args))
+        assert out["sat"] and out["verified"]
+        assign = np.array([1 if l > 0 else -1 for l in out["v"]], np.int8)
+        assert len(assign) == f["n"]
+
+
+def test_cli_reports_unknown_at_step_cap(tmp_path, fixtures):
+    f = fixtures["n1000"]
+    path = str(tmp_path / "n1000.cnf")
+    dmm.write_cnf(dmm.from_arrays(f["lits"], f["off"], f["n"]), path)
+    out = run_cli(["-i", path, "-l", "1", "-z", "5"])
+    assert "s [0] UNKNOWN" in out
+    assert not os.path.exists(path + ".solution.txt")
+
+
+def test_cli_rejects_long_clause(tmp_path):
+    path = tmp_path / "long.cnf"
+    path.write_text("p cnf 30 1\n" + " ".join(str(i) for i in range(1, 27)) + " 0\n")
+    r = subprocess.run([_lib.CLI_PATH, "-i", str(path)], capture_output=True, text=True)
+    assert r.returncode != 0
+    assert "MORE THAN 25 LITERALS" in r.stdout
