@@ -170,8 +170,8 @@ def peaks() -> tuple[float, str]:
 
 def profiled_traffic() -> float | None:
     """DRAM bytes per launch of the clause kernel at this workload, from the committed
-    ncu summary (profiles/k_clause_n100k.md, line `traffic_bytes_per_launch: X`)."""
-    p = os.path.join(ROOT, "profiles", "k_clause_n100k.md")
+    ncu summary (profiles/k_persist_n100k.md, line `traffic_bytes_per_launch: X`)."""
+    p = os.path.join(ROOT, "profiles", "k_persist_n100k.md")
     try:
         with open(p) as f:
             m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
