@@ -88,6 +88,7 @@ struct PackView {
   int32_t ring_cap;
   const int32_t* live;      // indices of the instances with tiles
   const int32_t* nlive;
+  const int32_t* upos;      // variable-major position of each slot (null: u is slot-major)
 };
 
 // ---- exactly rounded arithmetic (no FMA contraction: the reference has none) ----------

@@ -71,6 +71,8 @@ __global__ void __launch_bounds__(kInstThreads, 1)
     const InstDesc& I = sc.I;
     const int n = I.n, m = I.m;
     float* u = I.nslots <= kInstUCap ? sU : P.u + I.slot0;
+    // variable-major storage: contribution of slot s goes to u[upos[s]]
+    const int32_t* __restrict__ upos = P.upos ? P.upos + I.slot0 : nullptr;
     const int32_t* __restrict__ lit = P.lit + I.slot0;
     const int32_t* __restrict__ vsl = P.vslot + I.slot0;
     const int32_t* __restrict__ vend = P.vend + I.var0;
@@ -101,13 +103,20 @@ __global__ void __launch_bounds__(kInstThreads, 1)
           float u0, u1, u2;
           C = clause3(l0, l1, l2, sV[abs(l0) - 1], sV[abs(l1) - 1], sV[abs(l2) - 1], xs, xl, kc,
                       u0, u1, u2, ss);
-          u[3 * c] = u0;
-          u[3 * c + 1] = u1;
-          u[3 * c + 2] = u2;
+          if (upos) {
+            u[__ldg(upos + 3 * c)] = u0;
+            u[__ldg(upos + 3 * c + 1)] = u1;
+            u[__ldg(upos + 3 * c + 2)] = u2;
+          } else {
+            u[3 * c] = u0;
+            u[3 * c + 1] = u1;
+            u[3 * c + 2] = u2;
+          }
         } else {
           const int s0 = P.coff[I.cls0 + c];
           const int s1 = (c + 1 < m) ? P.coff[I.cls0 + c + 1] : I.nslots;
-          C = clause_general(lit + s0, s1 - s0, sV, xs, xl, kc, u + s0, ss);
+          C = clause_general(lit + s0, s1 - s0, sV, xs, xl, kc, upos ? u : u + s0,
+                             upos ? upos + s0 : nullptr, ss);
         }
         Xs[c] = xs;
         Xl[c] = xl;
@@ -151,10 +160,19 @@ __global__ void __launch_bounds__(kInstThreads, 1)
               vfail += !ss;
               e += (double)C * kEnergyUnitF32;
             }
-            float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
-            U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
-            U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
-            U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
+            if (upos) {
+              const int4* Q4 = reinterpret_cast<const int4*>(upos + 3 * g);
+              const int4 QA = __ldg(Q4), QB = __ldg(Q4 + 1), QC = __ldg(Q4 + 2);
+              const int Q[12] = {QA.x, QA.y, QA.z, QA.w, QB.x, QB.y,
+                                 QB.z, QB.w, QC.x, QC.y, QC.z, QC.w};
+#pragma unroll
+              for (int i = 0; i < 12; i++) u[Q[i]] = uu[i];
+            } else {
+              float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
+              U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
+              U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
+              U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
+            }
             *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
             *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
             *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
@@ -183,7 +201,8 @@ __global__ void __launch_bounds__(kInstThreads, 1)
           s1 = __ldg(vend + v);
           s0 = v > 0 ? __ldg(vend + v - 1) : 0;
         }
-        const float dv = tree_sum<float, G>(u, vsl + s0, s1 - s0, lane);
+        const float dv = upos ? tree_sum<float, G, true>(u + s0, nullptr, s1 - s0, lane)
+                              : tree_sum<float, G, false>(u, vsl + s0, s1 - s0, lane);
         if (valid && lane == 0) {
           sdV[v] = dv;
           const float V = sV[v];

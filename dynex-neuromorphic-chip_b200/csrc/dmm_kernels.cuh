@@ -128,11 +128,12 @@ __device__ __forceinline__ T clause3(int l0, int l1, int l2, T v0, T v1, T v2, T
 
 // General clause of k literals (2-SAT dynex.cc:420-454 and k-SAT dynex.cc:457-494 compute
 // the same values as this loop; k = 1 runs no branch, C = 0; k = 0 leaves C = INT_MAX/2).
+// Contribution j goes to u[upos[j]] (variable-major storage) or, with upos null, to u[j].
 template <class T>
 __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int k,
                                             const T* V, T Xs, T Xl,
                                             const ClauseConsts<T>& kc, T* __restrict__ u,
-                                            bool& strict_sat) {
+                                            const int32_t* __restrict__ upos, bool& strict_sat) {
   const T one = T(1), half = T(0.5), zero = T(0);
   strict_sat = false;
   if (k == 0) return mul(T(2147483647.0), half);
@@ -140,7 +141,7 @@ __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int
     const int l = __ldg(lit);
     const T v = V[abs(l) - 1];
     strict_sat = (v > zero && l > 0) || (v < zero && l < 0);
-    u[0] = zero;
+    u[upos ? __ldg(upos) : 0] = zero;
     return zero;
   }
   T a[kMaxK];
@@ -171,7 +172,7 @@ __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int
     const T others = (j == arg) ? mn2 : mn;
     const T g = mul(mul(q, others), half);
     const T r = (C == mul(a[j], half)) ? mul(sub(q, c), half) : zero;
-    u[j] = add(mul(xlxs, g), mul(rfac, r));
+    u[upos ? __ldg(upos + j) : j] = add(mul(xlxs, g), mul(rfac, r));
   }
   return C;
 }
@@ -183,7 +184,8 @@ __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int
 // combined by xor butterflies with offsets 16, 8, 4, 2, 1.  Lane `lane` of the group
 // holds virtual lanes lane + G*i; butterflies with offset >= G are lane-local, smaller
 // ones are shuffles.  Every G gives the same value.  All 32 lanes of the warp must call.
-template <class T, int G>
+// DIRECT: the d contributions are u[0..d) (variable-major storage); otherwise u[vs[j]].
+template <class T, int G, bool DIRECT = false>
 __device__ __forceinline__ T tree_sum(const T* u, const int32_t* __restrict__ vs,
                                       int d, int lane) {
   constexpr int NV = 32 / G;
@@ -194,7 +196,7 @@ __device__ __forceinline__ T tree_sum(const T* u, const int32_t* __restrict__ vs
 #pragma unroll
     for (int i = 0; i < NV; i++) {
       const int j = base + lane + G * i;
-      if (j < d) p[i] = add(p[i], u[__ldg(vs + j)]);
+      if (j < d) p[i] = add(p[i], DIRECT ? u[j] : u[__ldg(vs + j)]);
     }
   }
 #pragma unroll
@@ -213,7 +215,7 @@ __device__ __forceinline__ T tree_sum(const T* u, const int32_t* __restrict__ vs
 // Reference summation (dynex.cc:527-530): contributions sorted ascending, summed left to
 // right from +0.0 (zero contributions, which the reference skips, change no partial sum).
 // One warp per variable; d must be warp-uniform.  Bitonic sort in registers for d <= 32R.
-template <int R>
+template <int R, bool DIRECT>
 __device__ __forceinline__ double sorted_sum_reg(const double* u,
                                                  const int32_t* __restrict__ vs, int d,
                                                  int lane) {
@@ -222,7 +224,7 @@ __device__ __forceinline__ double sorted_sum_reg(const double* u,
 #pragma unroll
   for (int r = 0; r < R; r++) {
     const int j = r * 32 + lane;
-    a[r] = (j < d) ? u[__ldg(vs + j)] : pinf;
+    a[r] = (j < d) ? (DIRECT ? u[j] : u[__ldg(vs + j)]) : pinf;
   }
   constexpr int N = 32 * R;
 #pragma unroll
@@ -274,6 +276,7 @@ __device__ __forceinline__ double sorted_sum_reg(const double* u,
 static __device__ __noinline__ double sorted_sum_select(const double* u,
                                                  const int32_t* __restrict__ vs, int d,
                                                  int lane) {
+  // vs == nullptr: the contributions are u[0..d)
   double acc = 0.0;
   double lv = -inf_val<double>();
   int li = -1;
@@ -281,7 +284,7 @@ static __device__ __noinline__ double sorted_sum_select(const double* u,
     double bv = inf_val<double>();
     int bi = 0x7fffffff;
     for (int j = lane; j < d; j += 32) {
-      const double x = u[__ldg(vs + j)];
+      const double x = vs ? u[__ldg(vs + j)] : u[j];
       const bool after = (x > lv) || (x == lv && j > li);
       const bool better = (x < bv) || (x == bv && j < bi);
       if (after && better) {
@@ -305,13 +308,14 @@ static __device__ __noinline__ double sorted_sum_select(const double* u,
   return acc;
 }
 
+template <bool DIRECT = false>
 __device__ __forceinline__ double sorted_sum(const double* u,
                                              const int32_t* __restrict__ vs, int d, int lane) {
-  if (d <= 32) return sorted_sum_reg<1>(u, vs, d, lane);
-  if (d <= 64) return sorted_sum_reg<2>(u, vs, d, lane);
-  if (d <= 128) return sorted_sum_reg<4>(u, vs, d, lane);
-  if (d <= 256) return sorted_sum_reg<8>(u, vs, d, lane);
-  return sorted_sum_select(u, vs, d, lane);
+  if (d <= 32) return sorted_sum_reg<1, DIRECT>(u, vs, d, lane);
+  if (d <= 64) return sorted_sum_reg<2, DIRECT>(u, vs, d, lane);
+  if (d <= 128) return sorted_sum_reg<4, DIRECT>(u, vs, d, lane);
+  if (d <= 256) return sorted_sum_reg<8, DIRECT>(u, vs, d, lane);
+  return sorted_sum_select(u, DIRECT ? nullptr : vs, d, lane);
 }
 
 // ---- setup, state I/O and the reference function-pair mirrors ---------------------------
@@ -415,6 +419,13 @@ static __global__ void __launch_bounds__(kThreads) k_sort_lists(const int32_t* _
     for (int j = lane; j < d; j += 32) vslot[s0 + j] = buf[j];
     __syncwarp();
   }
+}
+
+// Position of each literal slot in the variable-major order: pos[vslot[j]] = j.
+static __global__ void k_invert(const int32_t* __restrict__ vslot, int nslots,
+                                int32_t* __restrict__ pos) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nslots; j += gridDim.x * blockDim.x)
+    pos[vslot[j]] = j;
 }
 
 // x (doubles, reference layout) -> V in cand[0][0], Xs, Xl.

@@ -169,6 +169,7 @@ class Pack {
   int32_t* coff_ = nullptr;
   int32_t* lit_ = nullptr;
   int32_t* vslot_ = nullptr;
+  int32_t* upos_ = nullptr;  // variable-major position of each slot
   int32_t* vend_ = nullptr;
   int32_t* fill_ = nullptr;
   int8_t* unit_ = nullptr;

@@ -104,6 +104,8 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
   const T* __restrict__ acm = I.has_alpha_cm ? P.alpha_cm + I.cls0 : nullptr;
   const int32_t* __restrict__ lit = P.lit + I.slot0;
   T* __restrict__ u = P.u + I.slot0;
+  // variable-major storage: contribution of slot s goes to u[upos[s]]
+  const int32_t* __restrict__ upos = P.upos ? P.upos + I.slot0 : nullptr;
   const int c_begin = sm.tile.begin, c_end = sm.tile.begin + sm.tile.count;
   // FP32: energy in exact integer units of 2^-25 (order-independent); FP64: plain sum
   const double escale = sizeof(T) == 4 ? kEnergyUnitF32 : 1.0;
@@ -120,13 +122,20 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
       T u0, u1, u2;
       C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1], xs, xl, kc, u0, u1,
                   u2, ss);
-      u[3 * c] = u0;
-      u[3 * c + 1] = u1;
-      u[3 * c + 2] = u2;
+      if (upos) {
+        u[__ldg(upos + 3 * c)] = u0;
+        u[__ldg(upos + 3 * c + 1)] = u1;
+        u[__ldg(upos + 3 * c + 2)] = u2;
+      } else {
+        u[3 * c] = u0;
+        u[3 * c + 1] = u1;
+        u[3 * c + 2] = u2;
+      }
     } else {
       const int s0 = P.coff[I.cls0 + c];
       const int s1 = (c + 1 < I.m) ? P.coff[I.cls0 + c + 1] : I.nslots;
-      C = clause_general(lit + s0, s1 - s0, V, xs, xl, kc, u + s0, ss);
+      C = clause_general(lit + s0, s1 - s0, V, xs, xl, kc, upos ? u : u + s0,
+                         upos ? upos + s0 : nullptr, ss);
     }
     Xs[c] = xs;
     Xl[c] = xl;
@@ -176,10 +185,18 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
           vfail += !ss;
           e += (double)C * escale;
         }
-        float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
-        U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
-        U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
-        U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
+        if (upos) {
+          const int4* Q4 = reinterpret_cast<const int4*>(upos + 3 * g);
+          const int4 QA = __ldg(Q4), QB = __ldg(Q4 + 1), QC = __ldg(Q4 + 2);
+          const int Q[12] = {QA.x, QA.y, QA.z, QA.w, QB.x, QB.y, QB.z, QB.w, QC.x, QC.y, QC.z, QC.w};
+#pragma unroll
+          for (int i = 0; i < 12; i++) u[Q[i]] = uu[i];
+        } else {
+          float4* U4 = reinterpret_cast<float4*>(u + 3 * g);
+          U4[0] = make_float4(uu[0], uu[1], uu[2], uu[3]);
+          U4[1] = make_float4(uu[4], uu[5], uu[6], uu[7]);
+          U4[2] = make_float4(uu[8], uu[9], uu[10], uu[11]);
+        }
         *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
         *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
         *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
@@ -239,9 +256,12 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
     }
     T dv;
     if constexpr (SORTED) {
-      dv = T(sorted_sum(reinterpret_cast<const double*>(u), vsl + s0, s1 - s0, lane));
+      const double* ud = reinterpret_cast<const double*>(u);
+      dv = P.upos ? T(sorted_sum<true>(ud + s0, nullptr, s1 - s0, lane))
+                  : T(sorted_sum<false>(ud, vsl + s0, s1 - s0, lane));
     } else {
-      dv = tree_sum<T, G>(u, vsl + s0, s1 - s0, lane);
+      dv = P.upos ? tree_sum<T, G, true>(u + s0, nullptr, s1 - s0, lane)
+                  : tree_sum<T, G, false>(u, vsl + s0, s1 - s0, lane);
     }
     if (valid && lane == 0) {
       if (MODE == 1) {

@@ -144,7 +144,8 @@ Pack::~Pack() {
                   coff_,    lit_,       vslot_,   vend_,       fill_,      unit_,
                   epart_,   inst_d_,    ctrl_d_,  ctiles_d_,   vtiles_d_,  ntiles_d_,
                   queue_d_, active_d_,  ring_d_,  ring_tail_d_, scan_tmp_, longv_d_,
-                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_, order_d_};
+                  stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_, order_d_,
+                  upos_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : ev_)
@@ -186,6 +187,7 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   DMM_CUDA(cudaMalloc(&coff_, C * 4));
   DMM_CUDA(cudaMalloc(&lit_, S * 4));
   DMM_CUDA(cudaMalloc(&vslot_, S * 4));
+  DMM_CUDA(cudaMalloc(&upos_, S * 4));
   DMM_CUDA(cudaMalloc(&u_, S * tsize_));
   DMM_CUDA(cudaMalloc(&cand_, 2 * kTrials * V * tsize_));
   DMM_CUDA(cudaMalloc(&vend_, V * 4));
@@ -251,6 +253,10 @@ dmm_status Pack::set_tuning(const dmm_tuning* t) {
   if (n.steps_per_graph > 4096) n.steps_per_graph = 4096;
   if (n.blocks_per_sm < 0 || n.blocks_per_sm > 32) {
     set_error("blocks_per_sm out of range");
+    return DMM_ERR_ARG;
+  }
+  if (n.u_layout < 0 || n.u_layout > 2) {
+    set_error("u_layout must be 0 (default), 1 (slot-major) or 2 (variable-major)");
     return DMM_ERR_ARG;
   }
   if (n.launch_mode < 0 || n.launch_mode > 3) {
@@ -387,6 +393,11 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
       std::sort(seg.begin(), seg.end());
       DMM_CUDA(cudaMemcpy(vsl + s0, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
     }
+  }
+  if (L > 0) {
+    // variable-major position of every slot (the inverse of the sorted CSR)
+    k_invert<<<blocks_for(L), kThreads, 0, stream_>>>(vsl, L, upos_ + I.slot0);
+    DMM_CUDA(cudaGetLastError());
   }
   (void)lits_host;
   return DMM_OK;
@@ -635,6 +646,7 @@ void Pack::fill_view(void* vv) const {
   v.ring_cap = caps_.insts;
   v.live = live_d_;
   v.nlive = misc_d_;
+  v.upos = tun_.u_layout == 1 ? nullptr : upos_;
 }
 
 dmm_status Pack::enqueue_clause() {

@@ -105,8 +105,15 @@ typedef struct dmm_tuning {
   int32_t var_tile;         /* variables per variable tile (>= 32; 0: as clause_tile)         */
   int32_t steps_per_graph;  /* steps per launch: per cooperative launch, or per CUDA graph   */
   int32_t blocks_per_sm;    /* two-kernel form: persistent blocks per SM (0: occupancy)      */
-  int32_t launch_mode;      /* 0: one cooperative launch runs steps_per_graph steps with grid
-                               barriers between phases; 1: one kernel per phase, CUDA graphs */
+  int32_t launch_mode;      /* 0: automatic (cooperative launches running steps_per_graph
+                               steps with grid barriers between phases; one block per small
+                               formula when there are enough of them); 1: one kernel per
+                               phase, CUDA graphs; 2: cooperative only; 3: one block per
+                               formula for every formula that fits                          */
+  int32_t u_layout;         /* storage of the per-literal contributions: 0 default
+                               (variable-major), 1 slot-major (gathered through the CSR),
+                               2 variable-major (scattered through the slot positions)       */
+  int32_t reserved;
 } dmm_tuning;
 
 /* A DIMACS formula held in host memory (allocated by the library). */

@@ -41,7 +41,7 @@ def test_abi_version_and_strings():
 def test_struct_sizes():
     assert ctypes.sizeof(_lib.Params) == 56
     assert ctypes.sizeof(_lib.Report) == 56
-    assert ctypes.sizeof(_lib.Tuning) == 24
+    assert ctypes.sizeof(_lib.Tuning) == 32
     assert ctypes.sizeof(_lib.Cnf) == 40
 
 

@@ -160,6 +160,27 @@ def test_fp32_launch_shape_does_not_change_results(fixtures):
         assert np.array_equal(x, outs[0][0])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_contribution_layout_does_not_change_results(fixtures, prec):
+    """Slot-major (gathered through the CSR) and variable-major (scattered through the slot
+    positions) storage of the per-literal contributions give identical states."""
+    f = fixtures["n500"]
+    x0 = uniform_init(f["n"], f["m"], 71)
+    outs = []
+    for lay, mode in ((1, 0), (2, 0), (1, 1), (2, 1), (2, 3), (1, 3)):
+        if prec == "fp64" and mode == 3:
+            continue
+        with dmm.Instance(formula(f), precision=prec) as inst:
+            inst.set_tuning(u_layout=lay, launch_mode=mode)
+            inst.set_state(x0)
+            inst.step(120)
+            d, loc, _ = inst.generate_dxdt(inst.get_state()[0])
+            outs.append((inst.get_state()[0], d, loc))
+    for x, d, loc in outs[1:]:
+        assert np.array_equal(x, outs[0][0])
+        assert np.array_equal(d, outs[0][1]) and loc == outs[0][2]
+
+
 def test_fp32_error_vs_fp64_per_horizon(fixtures):
     """Max |dV| and |dXl| of FP32 against FP64 from the same state, at steps 10 and 100
     (chaotic dynamics: the bound loosens with the horizon)."""
