@@ -646,7 +646,9 @@ void Pack::fill_view(void* vv) const {
   v.ring_cap = caps_.insts;
   v.live = live_d_;
   v.nlive = misc_d_;
-  v.upos = tun_.u_layout == 1 ? nullptr : upos_;
+  // tile paths: slot-major unless asked (measured faster there); the one-block-per-formula
+  // kernel switches to variable-major by default in launch_inst
+  v.upos = tun_.u_layout == 2 ? upos_ : nullptr;
 }
 
 dmm_status Pack::enqueue_clause() {
@@ -865,6 +867,9 @@ static dmm_status launch_inst_g(const PackView<float>& v, const int32_t* order, 
 dmm_status Pack::launch_inst(int32_t nsteps) {
   PackView<float> v;
   fill_view<float>(&v);
+  // variable-major contributions by default here: scattered into shared memory, then read
+  // contiguously per variable (measured 1.5x faster than gathering through the CSR)
+  v.upos = tun_.u_layout == 1 ? nullptr : upos_;
   int* queue = misc_d_ + 3;
   DMM_CUDA(cudaMemsetAsync(queue, 0, sizeof(int32_t), stream_));
   const int grid = std::max(1, std::min(sms_, (int)n_small_));

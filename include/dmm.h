@@ -110,9 +110,10 @@ typedef struct dmm_tuning {
                                formula when there are enough of them); 1: one kernel per
                                phase, CUDA graphs; 2: cooperative only; 3: one block per
                                formula for every formula that fits                          */
-  int32_t u_layout;         /* storage of the per-literal contributions: 0 default
-                               (variable-major), 1 slot-major (gathered through the CSR),
-                               2 variable-major (scattered through the slot positions)       */
+  int32_t u_layout;         /* storage of the per-literal contributions: 0 default (slot-major
+                               on the tile paths, variable-major in the one-block-per-formula
+                               kernel), 1 slot-major (gathered through the CSR), 2 variable-
+                               major (scattered through the slot positions)                  */
   int32_t reserved;
 } dmm_tuning;
 
