@@ -89,6 +89,15 @@ struct PackView {
   const int32_t* live;      // indices of the instances with tiles
   const int32_t* nlive;
   const int32_t* upos;      // variable-major position of each slot (null: u is slot-major)
+  // staged transpose of the contributions (single formula, cooperative launch); xspos null
+  // when inactive.  Block t stages its clause tile's contributions in shared memory
+  // grouped by destination variable tile and writes them to u[3 * tile begin ..); variable
+  // tile b gathers its chunks and reduces through xbidx.
+  const uint16_t* xspos;    // per slot: position in its clause tile's staging area
+  const uint16_t* xbidx;    // per variable-major position: position in its tile's bucket
+  const int32_t* xgoff;     // [b * nct + t]: local slot index of chunk (t, b) in u
+  const int32_t* xboff;     // [b * (nct + 1) + t]: offset of chunk (t, b) in bucket b
+  int32_t xnct;             // clause tiles (staging areas)
 };
 
 // ---- exactly rounded arithmetic (no FMA contraction: the reference has none) ----------

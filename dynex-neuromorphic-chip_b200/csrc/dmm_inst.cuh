@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kInstThreads, 1)
           s1 = __ldg(vend + v);
           s0 = v > 0 ? __ldg(vend + v - 1) : 0;
         }
-        const float dv = upos ? tree_sum<float, G, true>(u + s0, nullptr, s1 - s0, lane)
+        const float dv = upos ? tree_sum<float, G, true, int32_t>(u + s0, nullptr, s1 - s0, lane)
                               : tree_sum<float, G, false>(u, vsl + s0, s1 - s0, lane);
         if (valid && lane == 0) {
           sdV[v] = dv;

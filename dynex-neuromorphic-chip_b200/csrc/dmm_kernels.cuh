@@ -185,8 +185,8 @@ __device__ __forceinline__ T clause_general(const int32_t* __restrict__ lit, int
 // holds virtual lanes lane + G*i; butterflies with offset >= G are lane-local, smaller
 // ones are shuffles.  Every G gives the same value.  All 32 lanes of the warp must call.
 // DIRECT: the d contributions are u[0..d) (variable-major storage); otherwise u[vs[j]].
-template <class T, int G, bool DIRECT = false>
-__device__ __forceinline__ T tree_sum(const T* u, const int32_t* __restrict__ vs,
+template <class T, int G, bool DIRECT = false, class Idx = int32_t>
+__device__ __forceinline__ T tree_sum(const T* u, const Idx* __restrict__ vs,
                                       int d, int lane) {
   constexpr int NV = 32 / G;
   T p[NV];
@@ -215,9 +215,9 @@ __device__ __forceinline__ T tree_sum(const T* u, const int32_t* __restrict__ vs
 // Reference summation (dynex.cc:527-530): contributions sorted ascending, summed left to
 // right from +0.0 (zero contributions, which the reference skips, change no partial sum).
 // One warp per variable; d must be warp-uniform.  Bitonic sort in registers for d <= 32R.
-template <int R, bool DIRECT>
+template <int R, bool DIRECT, class Idx>
 __device__ __forceinline__ double sorted_sum_reg(const double* u,
-                                                 const int32_t* __restrict__ vs, int d,
+                                                 const Idx* __restrict__ vs, int d,
                                                  int lane) {
   double a[R];
   const double pinf = inf_val<double>();
@@ -273,8 +273,9 @@ __device__ __forceinline__ double sorted_sum_reg(const double* u,
 
 // Long lists: repeated selection of the next (value, position) pair in lexicographic
 // order; O(d^2 / 32) loads, no scratch memory.
-static __device__ __noinline__ double sorted_sum_select(const double* u,
-                                                 const int32_t* __restrict__ vs, int d,
+template <class Idx>
+__device__ __noinline__ double sorted_sum_select(const double* u,
+                                                 const Idx* __restrict__ vs, int d,
                                                  int lane) {
   // vs == nullptr: the contributions are u[0..d)
   double acc = 0.0;
@@ -308,14 +309,14 @@ static __device__ __noinline__ double sorted_sum_select(const double* u,
   return acc;
 }
 
-template <bool DIRECT = false>
+template <bool DIRECT = false, class Idx = int32_t>
 __device__ __forceinline__ double sorted_sum(const double* u,
-                                             const int32_t* __restrict__ vs, int d, int lane) {
-  if (d <= 32) return sorted_sum_reg<1, DIRECT>(u, vs, d, lane);
-  if (d <= 64) return sorted_sum_reg<2, DIRECT>(u, vs, d, lane);
-  if (d <= 128) return sorted_sum_reg<4, DIRECT>(u, vs, d, lane);
-  if (d <= 256) return sorted_sum_reg<8, DIRECT>(u, vs, d, lane);
-  return sorted_sum_select(u, DIRECT ? nullptr : vs, d, lane);
+                                             const Idx* __restrict__ vs, int d, int lane) {
+  if (d <= 32) return sorted_sum_reg<1, DIRECT, Idx>(u, vs, d, lane);
+  if (d <= 64) return sorted_sum_reg<2, DIRECT, Idx>(u, vs, d, lane);
+  if (d <= 128) return sorted_sum_reg<4, DIRECT, Idx>(u, vs, d, lane);
+  if (d <= 256) return sorted_sum_reg<8, DIRECT, Idx>(u, vs, d, lane);
+  return sorted_sum_select<Idx>(u, DIRECT ? nullptr : vs, d, lane);
 }
 
 // ---- setup, state I/O and the reference function-pair mirrors ---------------------------

@@ -138,6 +138,7 @@ class Pack {
   dmm_status capture(int32_t steps);
   dmm_status launch_persist(int32_t nsteps);
   dmm_status launch_inst(int32_t nsteps);
+  dmm_status prepare_xpose(int32_t idx, int TC, int TV, bool* ok);
   dmm_status ensure_flush(int64_t bytes);
   const void* persist_fn() const;
   dmm_status enqueue_step(bool rhs_only, void* dv_out);
@@ -170,6 +171,14 @@ class Pack {
   int32_t* lit_ = nullptr;
   int32_t* vslot_ = nullptr;
   int32_t* upos_ = nullptr;  // variable-major position of each slot
+  // staged transpose (single formula on the cooperative path)
+  bool xp_active_ = false;
+  uint16_t* xspos_ = nullptr;
+  uint16_t* xbidx_ = nullptr;
+  int32_t* xgoff_ = nullptr;
+  int32_t* xboff_ = nullptr;
+  int64_t xspos_cap_ = 0, xbidx_cap_ = 0, xgoff_cap_ = 0, xboff_cap_ = 0;
+  int32_t xnct_ = 0;
   int32_t* vend_ = nullptr;
   int32_t* fill_ = nullptr;
   int8_t* unit_ = nullptr;

@@ -90,8 +90,9 @@ __device__ __forceinline__ void load_tile(TileSmem<NT>& sm, const PackView<T>& P
 }
 
 // ---- phase A -------------------------------------------------------------------------------
-template <class T, bool VEC, int NT>
-__device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
+// XP: staged transpose (see PackView::xspos); `stage` is the block's shared-memory area.
+template <class T, bool VEC, int NT, bool XP = false>
+__device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* stage = nullptr) {
   if (sm.snap.done != 0) return;  // block-uniform
   const InstDesc& I = sm.inst;
   const ClauseConsts<T> kc = make_consts<T>(I, sm.snap.h);
@@ -122,7 +123,12 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
       T u0, u1, u2;
       C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1], xs, xl, kc, u0, u1,
                   u2, ss);
-      if (upos) {
+      if (XP) {
+        const uint16_t* xs3 = P.xspos + I.slot0 + 3 * c;
+        stage[__ldg(xs3)] = u0;
+        stage[__ldg(xs3 + 1)] = u1;
+        stage[__ldg(xs3 + 2)] = u2;
+      } else if (upos) {
         u[__ldg(upos + 3 * c)] = u0;
         u[__ldg(upos + 3 * c + 1)] = u1;
         u[__ldg(upos + 3 * c + 2)] = u2;
@@ -185,7 +191,13 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
           vfail += !ss;
           e += (double)C * escale;
         }
-        if (upos) {
+        if (XP) {
+          const ushort4* S4 = reinterpret_cast<const ushort4*>(P.xspos + I.slot0 + 3 * g);
+          const ushort4 SA = __ldg(S4), SB = __ldg(S4 + 1), SC = __ldg(S4 + 2);
+          const int Q[12] = {SA.x, SA.y, SA.z, SA.w, SB.x, SB.y, SB.z, SB.w, SC.x, SC.y, SC.z, SC.w};
+#pragma unroll
+          for (int i = 0; i < 12; i++) stage[Q[i]] = uu[i];
+        } else if (upos) {
           const int4* Q4 = reinterpret_cast<const int4*>(upos + 3 * g);
           const int4 QA = __ldg(Q4), QB = __ldg(Q4 + 1), QC = __ldg(Q4 + 2);
           const int Q[12] = {QA.x, QA.y, QA.z, QA.w, QB.x, QB.y, QB.z, QB.w, QC.x, QC.y, QC.z, QC.w};
@@ -212,7 +224,13 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
     sm.cnt[0][w] = unsat;
     sm.cnt[1][w] = vfail;
   }
-  const double et = block_sum<NT>(e, sm.red);
+  const double et = block_sum<NT>(e, sm.red);  // also completes the staging area
+  if (XP) {
+    // the tile's contributions, grouped by destination variable tile, to u[3 c_begin ..)
+    const int ns = 3 * (c_end - c_begin);
+    T* dst = u + 3 * c_begin;
+    for (int i = threadIdx.x; i < ns; i += NT) dst[i] = stage[i];
+  }
   if (threadIdx.x == 0) {
     int tu = 0, tv = 0;
 #pragma unroll
@@ -231,8 +249,11 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
 // ---- phase B -------------------------------------------------------------------------------
 // MODE 0: integration step (candidates, trial index).  MODE 1: right-hand side only (dV
 // to dv_out, local variable index).  Returns after a block-wide barrier.
-template <class T, int G, bool SORTED, int MODE, int NT>
-__device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restrict__ dv_out) {
+// XP: the tile's contributions arrive as chunks from every clause tile (see
+// PackView::xspos); `bucket` is the block's shared-memory area, `ti` the variable tile.
+template <class T, int G, bool SORTED, int MODE, int NT, bool XP = false>
+__device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restrict__ dv_out,
+                         T* bucket = nullptr, int ti = 0) {
   if (sm.snap.done != 0) return;  // block-uniform
   const InstDesc& I = sm.inst;
   const T* u = P.u + I.slot0;
@@ -245,6 +266,17 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
   constexpr int VPP = NT / G;
   const int grp = threadIdx.x / G, lane = threadIdx.x % G;
   const int v_end = sm.tile.begin + sm.tile.count;
+  if (XP) {
+    const int nct = P.xnct;
+    const int32_t* goff = P.xgoff + (int64_t)ti * nct;
+    const int32_t* boff = P.xboff + (int64_t)ti * (nct + 1);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int t = w; t < nct; t += NT / 32) {
+      const int g0 = __ldg(goff + t), o0 = __ldg(boff + t), len = __ldg(boff + t + 1) - o0;
+      for (int i = l; i < len; i += 32) bucket[o0 + i] = u[g0 + i];
+    }
+    __syncthreads();
+  }
   int kmax = 0;
   for (int vb = sm.tile.begin; vb < v_end; vb += VPP) {
     const int v = vb + grp;
@@ -255,12 +287,19 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
       s0 = v > 0 ? __ldg(vend + v - 1) : 0;
     }
     T dv;
-    if constexpr (SORTED) {
+    if constexpr (XP) {
+      const uint16_t* bx = P.xbidx + I.slot0 + s0;
+      if constexpr (SORTED)
+        dv = T(sorted_sum<false, uint16_t>(reinterpret_cast<const double*>(bucket), bx, s1 - s0,
+                                           lane));
+      else
+        dv = tree_sum<T, G, false, uint16_t>(bucket, bx, s1 - s0, lane);
+    } else if constexpr (SORTED) {
       const double* ud = reinterpret_cast<const double*>(u);
-      dv = P.upos ? T(sorted_sum<true>(ud + s0, nullptr, s1 - s0, lane))
+      dv = P.upos ? T(sorted_sum<true, int32_t>(ud + s0, nullptr, s1 - s0, lane))
                   : T(sorted_sum<false>(ud, vsl + s0, s1 - s0, lane));
     } else {
-      dv = P.upos ? tree_sum<T, G, true>(u + s0, nullptr, s1 - s0, lane)
+      dv = P.upos ? tree_sum<T, G, true, int32_t>(u + s0, nullptr, s1 - s0, lane)
                   : tree_sum<T, G, false>(u, vsl + s0, s1 - s0, lane);
     }
     if (valid && lane == 0) {
@@ -455,10 +494,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int& ta
 
 // nsteps integration steps in one cooperative launch.  Blocks own tiles statically
 // (tile ti -> block ti % gridDim.x); phases A | B | F are separated by grid barriers.
-template <class T, int G, bool SORTED, bool VEC, int NT>
+template <class T, int G, bool SORTED, bool VEC, int NT, bool XP = false>
 __global__ void __launch_bounds__(NT, 1)
     k_persist(PackView<T> P, int nsteps, unsigned int* bar, int* err) {
   __shared__ TileSmem<NT> sm;
+  extern __shared__ __align__(16) unsigned char xdyn[];  // staging area (XP only)
+  T* xarea = reinterpret_cast<T*>(xdyn);
   __shared__ int s_ok, s_active;
   unsigned int target = 0;
   const int nct = P.ntiles[0], nvt = P.ntiles[1], nlive = *P.nlive;
@@ -471,12 +512,12 @@ __global__ void __launch_bounds__(NT, 1)
     if (s_active <= 0) break;  // grid-uniform: read after a barrier, written before one
     for (int ti = blockIdx.x; ti < nct; ti += gridDim.x) {
       load_tile<T, NT>(sm, P, P.ctiles, ti);
-      clause_tile<T, VEC, NT>(P, sm, ti);
+      clause_tile<T, VEC, NT, XP>(P, sm, ti, xarea);
     }
     if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
     for (int ti = blockIdx.x; ti < nvt; ti += gridDim.x) {
       load_tile<T, NT>(sm, P, P.vtiles, ti);
-      var_tile<T, G, SORTED, 0, NT>(P, sm, nullptr);
+      var_tile<T, G, SORTED, 0, NT, XP>(P, sm, nullptr, xarea, ti);
     }
     if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
     for (int k = blockIdx.x; k < nlive; k += gridDim.x) {

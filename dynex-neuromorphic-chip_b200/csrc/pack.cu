@@ -121,6 +121,7 @@ inline int blocks_for(int64_t work, int per = kThreads, int cap = 148 * 16) {
 constexpr int kMinClauseTile = 256;  // smallest clause tile (bounds the tile tables)
 constexpr int kMinVarTile = 32;      // smallest variable tile
 constexpr int kPersistThreads = 1024;  // block size of the cooperative step kernel
+constexpr int64_t kXposeBytes = 192 * 1024;  // shared memory of the staged transpose
 }  // namespace
 
 int64_t Pack::bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
@@ -145,7 +146,7 @@ Pack::~Pack() {
                   epart_,   inst_d_,    ctrl_d_,  ctiles_d_,   vtiles_d_,  ntiles_d_,
                   queue_d_, active_d_,  ring_d_,  ring_tail_d_, scan_tmp_, longv_d_,
                   stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_, order_d_,
-                  upos_};
+                  upos_,    xspos_,     xbidx_,   xgoff_,      xboff_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : ev_)
@@ -256,7 +257,7 @@ dmm_status Pack::set_tuning(const dmm_tuning* t) {
     return DMM_ERR_ARG;
   }
   if (n.u_layout < 0 || n.u_layout > 2) {
-    set_error("u_layout must be 0 (default), 1 (slot-major) or 2 (variable-major)");
+    set_error("u_layout must be 0 (default), 1 (slot-major, no staging) or 2 (variable-major)");
     return DMM_ERR_ARG;
   }
   if (n.launch_mode < 0 || n.launch_mode > 3) {
@@ -649,6 +650,11 @@ void Pack::fill_view(void* vv) const {
   // tile paths: slot-major unless asked (measured faster there); the one-block-per-formula
   // kernel switches to variable-major by default in launch_inst
   v.upos = tun_.u_layout == 2 ? upos_ : nullptr;
+  v.xspos = xp_active_ ? xspos_ : nullptr;
+  v.xbidx = xbidx_;
+  v.xgoff = xgoff_;
+  v.xboff = xboff_;
+  v.xnct = xnct_;
 }
 
 dmm_status Pack::enqueue_clause() {
@@ -704,25 +710,109 @@ dmm_status Pack::enqueue_step(bool rhs_only, void* dv_out) {
   return DMM_OK;
 }
 
-static int occupancy_blocks(const void* fn, int threads) {
+static int occupancy_blocks(const void* fn, int threads, size_t smem = 0) {
   int b = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, 0) != cudaSuccess) {
+  if (smem > 0 &&
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, smem) != cudaSuccess) {
     cudaGetLastError();
     b = 4;
   }
   return std::max(1, b);
 }
 
-const void* Pack::persist_fn() const {
-  if (prec_ == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads>;
-  switch (tun_.var_group) {
-    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads>;
-    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads>;
-    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads>;
-    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads>;
-    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads>;
-    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads>;
+template <bool XP>
+static const void* persist_fn_x(dmm_precision prec, int G) {
+  if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads, XP>;
+  switch (G) {
+    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, XP>;
+    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, XP>;
+    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads, XP>;
+    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads, XP>;
+    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads, XP>;
+    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads, XP>;
   }
+}
+
+const void* Pack::persist_fn() const {
+  return xp_active_ ? persist_fn_x<true>(prec_, tun_.var_group)
+                    : persist_fn_x<false>(prec_, tun_.var_group);
+}
+
+// Staged transpose of the contributions for a single formula on the cooperative path:
+// with one clause tile and one variable tile per block, block t stages its tile's
+// contributions in shared memory grouped by destination variable tile (ascending slot within
+// each group) and writes the area to u[3 t TC ..); variable tile b then copies the chunk of
+// every clause tile into its shared memory (ascending slot overall) and reduces through xbidx.
+// The per-variable summation order is unchanged.
+dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
+  *ok = false;
+  const InstDesc& I = inst_h_[idx];
+  if (!I.k3) return DMM_OK;
+  const int m = I.m, n = I.n, L = I.nslots;
+  const int nct = (m + TC - 1) / TC, nvt = (n + TV - 1) / TV;
+  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_) return DMM_OK;
+  const int64_t cap = kXposeBytes / (int64_t)tsize_;
+  if (3 * (int64_t)TC > cap) return DMM_OK;
+  std::vector<int32_t> lits(L), vsl(L);
+  DMM_CUDA(cudaMemcpyAsync(lits.data(), lit_ + I.slot0, (size_t)L * 4, cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaMemcpyAsync(vsl.data(), vslot_ + I.slot0, (size_t)L * 4, cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  auto tile_of = [&](int s) { return (s / 3) / TC; };
+  auto bucket_of = [&](int s) { return (std::abs(lits[s]) - 1) / TV; };
+  std::vector<int32_t> cnt((size_t)nct * nvt, 0);
+  for (int s = 0; s < L; s++) cnt[(size_t)tile_of(s) * nvt + bucket_of(s)]++;
+  std::vector<int32_t> start((size_t)nct * nvt);
+  for (int t = 0; t < nct; t++) {
+    int32_t acc = 0;
+    for (int b = 0; b < nvt; b++) {
+      start[(size_t)t * nvt + b] = acc;
+      acc += cnt[(size_t)t * nvt + b];
+    }
+  }
+  std::vector<int32_t> goff((size_t)nvt * nct), boff((size_t)nvt * (nct + 1));
+  for (int b = 0; b < nvt; b++) {
+    int64_t acc = 0;
+    for (int t = 0; t < nct; t++) {
+      goff[(size_t)b * nct + t] = 3 * t * TC + start[(size_t)t * nvt + b];
+      boff[(size_t)b * (nct + 1) + t] = (int32_t)acc;
+      acc += cnt[(size_t)t * nvt + b];
+    }
+    if (acc > cap) return DMM_OK;  // bucket too large for shared memory
+    boff[(size_t)b * (nct + 1) + nct] = (int32_t)acc;
+  }
+  std::vector<uint16_t> spos(L), bidx(L);
+  {
+    std::vector<int32_t> cur(start);
+    for (int s = 0; s < L; s++) spos[s] = (uint16_t)cur[(size_t)tile_of(s) * nvt + bucket_of(s)]++;
+  }
+  for (int j = 0; j < L; j++) {
+    const int s = vsl[j], t = tile_of(s), b = bucket_of(s);
+    bidx[j] = (uint16_t)(boff[(size_t)b * (nct + 1) + t] + (spos[s] - start[(size_t)t * nvt + b]));
+  }
+  auto grow = [&](void** p, int64_t* cap_now, int64_t bytes) -> dmm_status {
+    if (bytes <= *cap_now) return DMM_OK;
+    if (*p) DMM_CUDA(cudaFree(*p));
+    *p = nullptr;
+    DMM_CUDA(cudaMalloc(p, bytes));
+    *cap_now = bytes;
+    return DMM_OK;
+  };
+  DMM_TRY(grow((void**)&xspos_, &xspos_cap_, (int64_t)caps_.slots * 2));
+  DMM_TRY(grow((void**)&xbidx_, &xbidx_cap_, (int64_t)caps_.slots * 2));
+  DMM_TRY(grow((void**)&xgoff_, &xgoff_cap_, (int64_t)goff.size() * 4));
+  DMM_TRY(grow((void**)&xboff_, &xboff_cap_, (int64_t)boff.size() * 4));
+  DMM_CUDA(cudaMemcpyAsync(xspos_ + I.slot0, spos.data(), (size_t)L * 2, cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaMemcpyAsync(xbidx_ + I.slot0, bidx.data(), (size_t)L * 2, cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaMemcpyAsync(xgoff_, goff.data(), goff.size() * 4, cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaMemcpyAsync(xboff_, boff.data(), boff.size() * 4, cudaMemcpyHostToDevice, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  xnct_ = nct;
+  *ok = true;
+  return DMM_OK;
 }
 
 dmm_status Pack::commit_tiles() {
@@ -806,6 +896,14 @@ dmm_status Pack::commit_tiles() {
     set_error("tile tables overflow");
     return DMM_ERR_BUDGET;
   }
+  // staged transpose: one formula, cooperative path, one tile of each kind per block
+  xp_active_ = false;
+  if (coop && live_list.size() == 1 && small_list.empty() && tun_.u_layout == 0 &&
+      tun_.clause_tile == 0 && tun_.var_tile == 0) {
+    const int32_t gp = occupancy_blocks(persist_fn_x<true>(prec_, tun_.var_group),
+                                        kPersistThreads, kXposeBytes) * sms_;
+    if (gp == grid_p_) DMM_TRY(prepare_xpose(live_list[0], TC, TV, &xp_active_));
+  }
   if (!ctiles_h_.empty())
     DMM_CUDA(cudaMemcpyAsync(ctiles_d_, ctiles_h_.data(), ctiles_h_.size() * sizeof(Tile),
                              cudaMemcpyHostToDevice, stream_));
@@ -845,8 +943,9 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
   int* err = misc_d_ + 1;
   DMM_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned int), stream_));
   void* args[] = {view, &nsteps, &bar, &err};
-  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(kPersistThreads), args, 0,
-                                       stream_));
+  const size_t smem = xp_active_ ? (size_t)kXposeBytes : 0;
+  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(kPersistThreads), args,
+                                       smem, stream_));
   return DMM_OK;
 }
 

@@ -167,7 +167,7 @@ def test_contribution_layout_does_not_change_results(fixtures, prec):
     f = fixtures["n500"]
     x0 = uniform_init(f["n"], f["m"], 71)
     outs = []
-    for lay, mode in ((1, 0), (2, 0), (1, 1), (2, 1), (2, 3), (1, 3)):
+    for lay, mode in ((0, 0), (1, 0), (2, 0), (1, 1), (2, 1), (2, 3), (1, 3)):
         if prec == "fp64" and mode == 3:
             continue
         with dmm.Instance(formula(f), precision=prec) as inst:
