@@ -34,6 +34,8 @@
 namespace dmm {
 
 constexpr double kEnergyUnitF32 = 33554432.0;  // 2^25: every FP32 C_m is a multiple of 2^-25
+constexpr int kXpMaxChunks = 256;  // clause tiles the staged transpose supports
+constexpr int kXpUnroll = 8;       // independent loads per thread in the bucket copy
 
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -267,13 +269,38 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
   const int grp = threadIdx.x / G, lane = threadIdx.x % G;
   const int v_end = sm.tile.begin + sm.tile.count;
   if (XP) {
+    // flat copy of the bucket: position p lies in chunk t with boff[t] <= p < boff[t + 1];
+    // every thread keeps kXpUnroll independent loads in flight
+    __shared__ int32_t s_boff[kXpMaxChunks + 1], s_goff[kXpMaxChunks];
     const int nct = P.xnct;
     const int32_t* goff = P.xgoff + (int64_t)ti * nct;
     const int32_t* boff = P.xboff + (int64_t)ti * (nct + 1);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    for (int t = w; t < nct; t += NT / 32) {
-      const int g0 = __ldg(goff + t), o0 = __ldg(boff + t), len = __ldg(boff + t + 1) - o0;
-      for (int i = l; i < len; i += 32) bucket[o0 + i] = u[g0 + i];
+    for (int t = threadIdx.x; t <= nct; t += NT) {
+      s_boff[t] = __ldg(boff + t);
+      if (t < nct) s_goff[t] = __ldg(goff + t);
+    }
+    __syncthreads();
+    const int total = s_boff[nct];
+    for (int p0 = threadIdx.x; p0 < total; p0 += kXpUnroll * NT) {
+      T val[kXpUnroll];
+#pragma unroll
+      for (int k = 0; k < kXpUnroll; k++) {
+        const int p = p0 + k * NT;
+        if (p < total) {
+          int lo = 0, hi = nct;  // s_boff[lo] <= p < s_boff[hi]
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_boff[mid] <= p) lo = mid;
+            else hi = mid;
+          }
+          val[k] = u[s_goff[lo] + (p - s_boff[lo])];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kXpUnroll; k++) {
+        const int p = p0 + k * NT;
+        if (p < total) bucket[p] = val[k];
+      }
     }
     __syncthreads();
   }

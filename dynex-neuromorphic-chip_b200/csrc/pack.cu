@@ -754,7 +754,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   if (!I.k3) return DMM_OK;
   const int m = I.m, n = I.n, L = I.nslots;
   const int nct = (m + TC - 1) / TC, nvt = (n + TV - 1) / TV;
-  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_) return DMM_OK;
+  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_ || nct > kXpMaxChunks) return DMM_OK;
   const int64_t cap = kXposeBytes / (int64_t)tsize_;
   if (3 * (int64_t)TC > cap) return DMM_OK;
   std::vector<int32_t> lits(L), vsl(L);
