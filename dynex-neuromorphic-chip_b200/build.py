@@ -26,7 +26,7 @@ LIB = os.path.join(LIB_DIR, "libdmm.so")
 CLI = os.path.join(BIN_DIR, "dynex")
 
 SOURCES = ["pack.cu", "cnf.cpp", "capi.cpp", "server.cpp", "noalloc.cu"]
-HEADERS = ["dmm_device.cuh", "dmm_kernels.cuh", "dmm_step.cuh", "dmm_pack.h"]
+HEADERS = ["dmm_device.cuh", "dmm_kernels.cuh", "dmm_step.cuh", "dmm_inst.cuh", "dmm_pack.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -258,6 +258,12 @@ dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
   return inst->pack->time_steps_flushed(nsteps, flush_bytes, ms);
 }
 
+dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double* out) {
+  dmm::clear_error();
+  if (!inst || nsteps <= 0 || !out) return DMM_ERR_ARG;
+  return inst->pack->trace_phases(nsteps, out);
+}
+
 // ---- batch ---------------------------------------------------------------------------------
 
 dmm_status dmm_batch_create(dmm_precision precision, int32_t device, int32_t max_instances,

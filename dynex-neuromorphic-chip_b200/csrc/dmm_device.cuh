@@ -19,6 +19,7 @@ constexpr int kMaxK = 25;          // longest clause (MAX_LITS_SYSTEM, dynex.cc:
 constexpr int kThreads = 256;      // block size of every tile kernel (fixed: reductions
                                    // over a block are part of the result definition)
 constexpr int kTrials = 4;         // adaptive trials h = 1/8, 1/16, 1/32, 1/64
+constexpr int kTraceK = 10;        // trace points per step of the cooperative kernel
 
 // Read-only description of one instance.
 struct InstDesc {
@@ -52,6 +53,13 @@ struct InstCtrl {
   double best_t;
   // per-step accumulators, zeroed by the finalize step
   int32_t acc_loc, acc_vfail, acc_kmax, vtiles_done;
+};
+
+// Accumulators of one step of a single formula on the cooperative form (two per formula,
+// alternating by step): every block reads them after the step's last grid barrier.
+struct StepAcc {
+  int32_t loc, vfail, kmax, pad;
+  unsigned long long energy;  // FP32 energy in units of 2^-25 (exact)
 };
 
 struct Tile {
@@ -89,15 +97,31 @@ struct PackView {
   const int32_t* live;      // indices of the instances with tiles
   const int32_t* nlive;
   const int32_t* upos;      // variable-major position of each slot (null: u is slot-major)
-  // staged transpose of the contributions (single formula, cooperative launch); xspos null
-  // when inactive.  Block t stages its clause tile's contributions in shared memory
-  // grouped by destination variable tile and writes them to u[3 * tile begin ..); variable
-  // tile b gathers its chunks and reduces through xbidx.
-  const uint16_t* xspos;    // per slot: position in its clause tile's staging area
-  const uint16_t* xbidx;    // per variable-major position: position in its tile's bucket
-  const int32_t* xgoff;     // [b * nct + t]: local slot index of chunk (t, b) in u
-  const int32_t* xboff;     // [b * (nct + 1) + t]: offset of chunk (t, b) in bucket b
-  int32_t xnct;             // clause tiles (staging areas)
+  StepAcc* acc2;            // [2] step accumulators of the single-formula cooperative form
+  // staged form (FP32, one formula of 3-literal clauses, cooperative launch, one clause
+  // tile and one variable tile per block; xdlist null when off).  Clause tile t gathers
+  // the voltages of its distinct variables xdlist[xdoff[t] ..) into shared memory, reads
+  // them through the tile-local literals xllit (+-(1 + position in the list)), stages each
+  // contribution at xspos in a shared area grouped by destination variable tile (chunks
+  // padded to 8 entries) and writes the area to ux[xubase[t] ..).  Variable tile b reads
+  // bucket positions [xboff[b], xboff[b + 1]) (ux index of every 8 positions in xsrc8)
+  // and scatters them to their variable-major positions xdst in shared memory.
+  const int32_t* xdlist;
+  const int32_t* xdoff;     // [clause tiles + 1]
+  const int16_t* xllit;     // per slot of the formula
+  const uint16_t* xspos;    // per slot of the formula
+  T* ux;
+  const int32_t* xubase;    // [clause tiles + 1], multiples of 8
+  const int32_t* xboff;     // [variable tiles + 1], multiples of 8
+  const int32_t* xsrc8;     // per 8 bucket positions
+  const uint16_t* xdst;     // per bucket position; 0xFFFF for padding
+  int32_t xsv_cap, xbk_cap, xtv_cap;  // shared-memory capacities (entries)
+  // phase trace of the cooperative kernel (null when off): trace[(s * kTraceK + k) * grid +
+  // block] = %globaltimer at step s's point k: 0 start, 1 clause tile loaded, 2 voltages
+  // gathered, 3 phase A done, 4 past barrier 1, 5 variable tile loaded, 6 bucket filled,
+  // 7 phase B done, 8 past barrier 2, 9 phase F done
+  long long* trace;
+  int32_t trace_steps;
 };
 
 // ---- exactly rounded arithmetic (no FMA contraction: the reference has none) ----------

@@ -105,6 +105,10 @@ class Pack {
   dmm_status profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t);
   // nsteps steps each launched alone after an L2 flush; summed device time of the steps.
   dmm_status time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double* ms);
+  // One cooperative launch of nsteps steps with %globaltimer stamps at kTraceK points of
+  // every step; out[2k], out[2k+1] = mean and max over blocks of the microseconds from
+  // point k to point k+1 (point kTraceK: the next step's start), averaged over steps.
+  dmm_status trace_phases(int32_t nsteps, double* out);
   // Raises DMM_ERR_CUDA when a cooperative launch reported a grid-barrier timeout.
   dmm_status check_error();
   dmm_status read_active(int32_t* active);
@@ -171,14 +175,17 @@ class Pack {
   int32_t* lit_ = nullptr;
   int32_t* vslot_ = nullptr;
   int32_t* upos_ = nullptr;  // variable-major position of each slot
-  // staged transpose (single formula on the cooperative path)
+  // staged form (single FP32 formula of 3-literal clauses on the cooperative path)
   bool xp_active_ = false;
-  uint16_t* xspos_ = nullptr;
-  uint16_t* xbidx_ = nullptr;
-  int32_t* xgoff_ = nullptr;
-  int32_t* xboff_ = nullptr;
-  int64_t xspos_cap_ = 0, xbidx_cap_ = 0, xgoff_cap_ = 0, xboff_cap_ = 0;
-  int32_t xnct_ = 0;
+  bool one_active_ = false;  // single FP32 formula on the cooperative path
+  enum { kXpDlist, kXpDoff, kXpLlit, kXpSpos, kXpUx, kXpUbase, kXpBoff, kXpSrc8, kXpDst, kXpBufs };
+  void* xbuf_[kXpBufs] = {};
+  int64_t xbuf_cap_[kXpBufs] = {};
+  int32_t xsv_cap_ = 0, xbk_cap_ = 0, xtv_cap_ = 0, xsmem_ = 0;
+  long long* trace_ = nullptr;
+  int64_t trace_cap_ = 0;
+  bool trace_on_ = false;
+  int32_t trace_steps_ = 0;
   int32_t* vend_ = nullptr;
   int32_t* fill_ = nullptr;
   int8_t* unit_ = nullptr;

@@ -34,8 +34,6 @@
 namespace dmm {
 
 constexpr double kEnergyUnitF32 = 33554432.0;  // 2^25: every FP32 C_m is a multiple of 2^-25
-constexpr int kXpMaxChunks = 256;  // clause tiles the staged transpose supports
-constexpr int kXpUnroll = 8;       // independent loads per thread in the bucket copy
 
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -52,6 +50,16 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return r;
 }
 
+// Records %globaltimer at trace point k of step s (thread 0; no-op unless tracing).
+template <class T>
+__device__ __forceinline__ void trace_stamp(const PackView<T>& P, int s, int k) {
+  if (P.trace && threadIdx.x == 0 && s < P.trace_steps) {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    P.trace[((int64_t)s * kTraceK + k) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
 struct TileSnap {
   int32_t done, pending, set, kcur;
   double h;
@@ -63,6 +71,7 @@ struct TileSmem {
   TileSnap snap;
   Tile tile;
   int cached;  // instance whose description + snapshot are loaded, -1 for none
+  StepAcc* acc;  // step accumulators (single-formula cooperative form), else null
   int ti;
   int flag;
   double red[NT / 32];
@@ -91,10 +100,26 @@ __device__ __forceinline__ void load_tile(TileSmem<NT>& sm, const PackView<T>& P
   __syncthreads();
 }
 
+// Adds a clause tile's unsatisfied count, strict-sign failures and energy partial to the
+// step's accumulators (thread 0).
+template <class T, int NT>
+__device__ __forceinline__ void add_clause_counts(const PackView<T>& P, TileSmem<NT>& sm, int ti,
+                                                  int tu, int tv, double et) {
+  if (sm.acc) {
+    if (tu) atomicAdd(&sm.acc->loc, tu);
+    if (tv) atomicAdd(&sm.acc->vfail, tv);
+    atomicAdd(&sm.acc->energy, (unsigned long long)et);  // FP32: exact integer units
+  } else {
+    InstCtrl* S = P.ctrl + sm.tile.inst;
+    if (tu) atomicAdd(&S->acc_loc, tu);
+    if (tv) atomicAdd(&S->acc_vfail, tv);
+    P.epart[ti] = et;
+  }
+}
+
 // ---- phase A -------------------------------------------------------------------------------
-// XP: staged transpose (see PackView::xspos); `stage` is the block's shared-memory area.
-template <class T, bool VEC, int NT, bool XP = false>
-__device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* stage = nullptr) {
+template <class T, bool VEC, int NT>
+__device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti) {
   if (sm.snap.done != 0) return;  // block-uniform
   const InstDesc& I = sm.inst;
   const ClauseConsts<T> kc = make_consts<T>(I, sm.snap.h);
@@ -125,12 +150,7 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* s
       T u0, u1, u2;
       C = clause3(l0, l1, l2, V[abs(l0) - 1], V[abs(l1) - 1], V[abs(l2) - 1], xs, xl, kc, u0, u1,
                   u2, ss);
-      if (XP) {
-        const uint16_t* xs3 = P.xspos + I.slot0 + 3 * c;
-        stage[__ldg(xs3)] = u0;
-        stage[__ldg(xs3 + 1)] = u1;
-        stage[__ldg(xs3 + 2)] = u2;
-      } else if (upos) {
+      if (upos) {
         u[__ldg(upos + 3 * c)] = u0;
         u[__ldg(upos + 3 * c + 1)] = u1;
         u[__ldg(upos + 3 * c + 2)] = u2;
@@ -193,13 +213,7 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* s
           vfail += !ss;
           e += (double)C * escale;
         }
-        if (XP) {
-          const ushort4* S4 = reinterpret_cast<const ushort4*>(P.xspos + I.slot0 + 3 * g);
-          const ushort4 SA = __ldg(S4), SB = __ldg(S4 + 1), SC = __ldg(S4 + 2);
-          const int Q[12] = {SA.x, SA.y, SA.z, SA.w, SB.x, SB.y, SB.z, SB.w, SC.x, SC.y, SC.z, SC.w};
-#pragma unroll
-          for (int i = 0; i < 12; i++) stage[Q[i]] = uu[i];
-        } else if (upos) {
+        if (upos) {
           const int4* Q4 = reinterpret_cast<const int4*>(upos + 3 * g);
           const int4 QA = __ldg(Q4), QB = __ldg(Q4 + 1), QC = __ldg(Q4 + 2);
           const int Q[12] = {QA.x, QA.y, QA.z, QA.w, QB.x, QB.y, QB.z, QB.w, QC.x, QC.y, QC.z, QC.w};
@@ -226,13 +240,7 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* s
     sm.cnt[0][w] = unsat;
     sm.cnt[1][w] = vfail;
   }
-  const double et = block_sum<NT>(e, sm.red);  // also completes the staging area
-  if (XP) {
-    // the tile's contributions, grouped by destination variable tile, to u[3 c_begin ..)
-    const int ns = 3 * (c_end - c_begin);
-    T* dst = u + 3 * c_begin;
-    for (int i = threadIdx.x; i < ns; i += NT) dst[i] = stage[i];
-  }
+  const double et = block_sum<NT>(e, sm.red);
   if (threadIdx.x == 0) {
     int tu = 0, tv = 0;
 #pragma unroll
@@ -240,10 +248,7 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* s
       tu += sm.cnt[0][i];
       tv += sm.cnt[1][i];
     }
-    InstCtrl* S = P.ctrl + sm.tile.inst;
-    if (tu) atomicAdd(&S->acc_loc, tu);
-    if (tv) atomicAdd(&S->acc_vfail, tv);
-    P.epart[ti] = et;
+    add_clause_counts(P, sm, ti, tu, tv, et);
   }
   __syncthreads();
 }
@@ -251,11 +256,8 @@ __device__ void clause_tile(const PackView<T>& P, TileSmem<NT>& sm, int ti, T* s
 // ---- phase B -------------------------------------------------------------------------------
 // MODE 0: integration step (candidates, trial index).  MODE 1: right-hand side only (dV
 // to dv_out, local variable index).  Returns after a block-wide barrier.
-// XP: the tile's contributions arrive as chunks from every clause tile (see
-// PackView::xspos); `bucket` is the block's shared-memory area, `ti` the variable tile.
-template <class T, int G, bool SORTED, int MODE, int NT, bool XP = false>
-__device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restrict__ dv_out,
-                         T* bucket = nullptr, int ti = 0) {
+template <class T, int G, bool SORTED, int MODE, int NT>
+__device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restrict__ dv_out) {
   if (sm.snap.done != 0) return;  // block-uniform
   const InstDesc& I = sm.inst;
   const T* u = P.u + I.slot0;
@@ -268,42 +270,6 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
   constexpr int VPP = NT / G;
   const int grp = threadIdx.x / G, lane = threadIdx.x % G;
   const int v_end = sm.tile.begin + sm.tile.count;
-  if (XP) {
-    // flat copy of the bucket: position p lies in chunk t with boff[t] <= p < boff[t + 1];
-    // every thread keeps kXpUnroll independent loads in flight
-    __shared__ int32_t s_boff[kXpMaxChunks + 1], s_goff[kXpMaxChunks];
-    const int nct = P.xnct;
-    const int32_t* goff = P.xgoff + (int64_t)ti * nct;
-    const int32_t* boff = P.xboff + (int64_t)ti * (nct + 1);
-    for (int t = threadIdx.x; t <= nct; t += NT) {
-      s_boff[t] = __ldg(boff + t);
-      if (t < nct) s_goff[t] = __ldg(goff + t);
-    }
-    __syncthreads();
-    const int total = s_boff[nct];
-    for (int p0 = threadIdx.x; p0 < total; p0 += kXpUnroll * NT) {
-      T val[kXpUnroll];
-#pragma unroll
-      for (int k = 0; k < kXpUnroll; k++) {
-        const int p = p0 + k * NT;
-        if (p < total) {
-          int lo = 0, hi = nct;  // s_boff[lo] <= p < s_boff[hi]
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_boff[mid] <= p) lo = mid;
-            else hi = mid;
-          }
-          val[k] = u[s_goff[lo] + (p - s_boff[lo])];
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < kXpUnroll; k++) {
-        const int p = p0 + k * NT;
-        if (p < total) bucket[p] = val[k];
-      }
-    }
-    __syncthreads();
-  }
   int kmax = 0;
   for (int vb = sm.tile.begin; vb < v_end; vb += VPP) {
     const int v = vb + grp;
@@ -314,14 +280,7 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
       s0 = v > 0 ? __ldg(vend + v - 1) : 0;
     }
     T dv;
-    if constexpr (XP) {
-      const uint16_t* bx = P.xbidx + I.slot0 + s0;
-      if constexpr (SORTED)
-        dv = T(sorted_sum<false, uint16_t>(reinterpret_cast<const double*>(bucket), bx, s1 - s0,
-                                           lane));
-      else
-        dv = tree_sum<T, G, false, uint16_t>(bucket, bx, s1 - s0, lane);
-    } else if constexpr (SORTED) {
+    if constexpr (SORTED) {
       const double* ud = reinterpret_cast<const double*>(u);
       dv = P.upos ? T(sorted_sum<true, int32_t>(ud + s0, nullptr, s1 - s0, lane))
                   : T(sorted_sum<false>(ud, vsl + s0, s1 - s0, lane));
@@ -358,13 +317,74 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
       int km = 0;
 #pragma unroll
       for (int i = 0; i < NT / 32; i++) km = max(km, sm.cnt[0][i]);
-      if (km) atomicMax(&P.ctrl[sm.tile.inst].acc_kmax, km);
+      if (km) atomicMax(sm.acc ? &sm.acc->kmax : &P.ctrl[sm.tile.inst].acc_kmax, km);
     }
   }
   __syncthreads();
 }
 
 // ---- phase F -------------------------------------------------------------------------------
+// The reference's step decision (dynex.cc:1389-1417) from a step's accumulators: accepted
+// trial, h of the deferred memory update, time advance, status after the step.
+struct StepDecision {
+  int kacc;   // trial slot of the accepted candidates
+  double hs;  // h of the accepted trial (1/64 when none passed)
+  double ht;  // time advance (1/128 when none passed)
+  int status; // 0 running, 1 solved, 2 step limit
+};
+
+__device__ __forceinline__ StepDecision decide(int loc, int vfail, int kmax, int step,
+                                               int max_steps) {
+  StepDecision d;
+  d.kacc = kmax < kTrials - 1 ? kmax : kTrials - 1;
+  d.hs = 0.125 / (double)(1 << d.kacc);
+  d.ht = kmax < kTrials ? d.hs : 0.0078125;
+  d.status = (loc == 0 && vfail == 0) ? 1 : (max_steps > 0 && step + 1 >= max_steps) ? 2 : 0;
+  return d;
+}
+
+// Writes the control state after step S->step of instance ii (one thread).
+template <class T>
+__device__ void commit_step(const PackView<T>& P, const InstDesc& I, int ii, int loc, int vfail,
+                            int kmax, double e) {
+  InstCtrl* S = P.ctrl + ii;
+  volatile InstCtrl* vS = S;
+  InstCtrl c;
+  // one burst of loads, then one burst of stores
+  c.step = vS->step;
+  c.set = vS->set;
+  c.kcur = vS->kcur;
+  c.best_loc = vS->best_loc;
+  c.t = vS->t;
+  c.best_t = vS->best_t;
+  const StepDecision d = decide(loc, vfail, kmax, c.step, I.max_steps);
+  if (loc < c.best_loc) {
+    S->best_loc = loc;
+    S->best_t = c.t;
+  }
+  if (d.status == 1) {
+    S->solved_step = c.step;
+    S->solved_t = c.t;
+    S->sol_set = c.set;
+    S->sol_k = c.kcur;
+  }
+  S->loc = loc;
+  S->vfail = vfail;
+  S->energy = e;
+  S->t = __dadd_rn(c.t, d.ht);
+  S->step = c.step + 1;
+  S->set = c.set ^ 1;
+  S->kcur = d.kacc;
+  S->h_state = d.hs;
+  S->pending = 1;
+  if (d.status) {
+    S->done = d.status;
+    atomicSub(P.active, 1);
+    const int pos = atomicAdd(P.ring_tail, 1);
+    P.ring[pos % P.ring_cap] = ii;
+  }
+}
+
 // Finalizes one instance's step (block-wide).  Reads the accumulators of the step, writes
 // the new control state, zeroes the accumulators.
 template <class T, int NT>
@@ -376,53 +396,14 @@ __device__ void finalize_step(const PackView<T>& P, const InstDesc& I, int ii, d
     if (sizeof(T) == 4) e = e * (1.0 / kEnergyUnitF32);
     InstCtrl* S = P.ctrl + ii;
     volatile InstCtrl* vS = S;
-    InstCtrl c;
-    // one burst of loads, then one burst of stores
-    c.step = vS->step;
-    c.set = vS->set;
-    c.kcur = vS->kcur;
-    c.best_loc = vS->best_loc;
-    c.t = vS->t;
-    c.best_t = vS->best_t;
     const int loc = vS->acc_loc;
     const int vfail = vS->acc_vfail;
     const int kmax = vS->acc_kmax;
-    const bool solved = (loc == 0 && vfail == 0);
-    const int kacc = kmax < kTrials - 1 ? kmax : kTrials - 1;
-    const double hs = 0.125 / (double)(1 << kacc);
-    const double ht = kmax < kTrials ? hs : 0.0078125;
-    if (loc < c.best_loc) {
-      S->best_loc = loc;
-      S->best_t = c.t;
-    }
-    if (solved) {
-      S->solved_step = c.step;
-      S->solved_t = c.t;
-      S->sol_set = c.set;
-      S->sol_k = c.kcur;
-    }
-    S->loc = loc;
-    S->vfail = vfail;
-    S->energy = e;
-    S->t = __dadd_rn(c.t, ht);
-    S->step = c.step + 1;
-    S->set = c.set ^ 1;
-    S->kcur = kacc;
-    S->h_state = hs;
-    S->pending = 1;
+    commit_step(P, I, ii, loc, vfail, kmax, e);
     S->acc_loc = 0;
     S->acc_vfail = 0;
     S->acc_kmax = 0;
     S->vtiles_done = 0;
-    int st = 0;
-    if (solved) st = 1;
-    else if (I.max_steps > 0 && c.step + 1 >= I.max_steps) st = 2;
-    if (st) {
-      S->done = st;
-      atomicSub(P.active, 1);
-      const int pos = atomicAdd(P.ring_tail, 1);
-      P.ring[pos % P.ring_cap] = ii;
-    }
     __threadfence();
   }
 }
@@ -434,6 +415,7 @@ __global__ void __launch_bounds__(kThreads) k_clause(PackView<T> P) {
   __shared__ TileSmem<kThreads> sm;
   if (threadIdx.x == 0) {
     sm.cached = -1;
+    sm.acc = nullptr;
     if (blockIdx.x == 0) P.queue[1] = 0;  // the variable-tile queue is idle
   }
   const int ntiles = P.ntiles[0];
@@ -452,6 +434,7 @@ __global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restr
   __shared__ TileSmem<kThreads> sm;
   if (threadIdx.x == 0) {
     sm.cached = -1;
+    sm.acc = nullptr;
     if (blockIdx.x == 0) P.queue[0] = 0;  // the clause-tile queue is idle
   }
   const int ntiles = P.ntiles[1];
@@ -479,6 +462,12 @@ __global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restr
     }
   }
 }
+
+}  // namespace dmm
+
+#include "dmm_xpose.cuh"
+
+namespace dmm {
 
 // ---- persistent form -------------------------------------------------------------------------
 
@@ -519,46 +508,155 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int& ta
   return *s_ok != 0;
 }
 
+// Tile load of the single-formula form: description loaded once per launch, snapshot from
+// the block's own copy of the control state.
+struct LocalSnap {
+  int done, step, set, kcur, pending;
+  double h;
+};
+
+template <int NT>
+__device__ __forceinline__ void load_tile_one(TileSmem<NT>& sm, const LocalSnap& ls,
+                                              const Tile* tiles, int ti) {
+  if (threadIdx.x == 0) {
+    sm.tile = tiles[ti];
+    sm.snap.done = ls.done;
+    sm.snap.pending = ls.pending;
+    sm.snap.set = ls.set;
+    sm.snap.kcur = ls.kcur;
+    sm.snap.h = ls.h;
+  }
+  __syncthreads();
+}
+
 // nsteps integration steps in one cooperative launch.  Blocks own tiles statically
 // (tile ti -> block ti % gridDim.x); phases A | B | F are separated by grid barriers.
-template <class T, int G, bool SORTED, bool VEC, int NT, bool XP = false>
+// ONE (a single FP32 formula): two grid barriers per step.  The step's counts go to the
+// accumulators acc2[s & 1] (zeroed before the launch; slot (s+1) & 1 is zeroed by block 0
+// once barrier 1 of step s has passed, after every block has read it in step s-1); after
+// barrier 2 every block reads them and applies the step decision to its own copy of the
+// control state, and block 0 writes the control state for the host.
+// XP: the staged form (implies ONE; clause tile and variable tile b belong to block b).
+template <class T, int G, bool SORTED, bool VEC, int NT, bool XP = false, bool ONE = false>
 __global__ void __launch_bounds__(NT, 1)
     k_persist(PackView<T> P, int nsteps, unsigned int* bar, int* err) {
+  static_assert(!XP || ONE, "the staged form runs with one formula");
   __shared__ TileSmem<NT> sm;
-  extern __shared__ __align__(16) unsigned char xdyn[];  // staging area (XP only)
-  T* xarea = reinterpret_cast<T*>(xdyn);
+  extern __shared__ __align__(16) unsigned char xdyn[];  // staged form only
+  __shared__ XpTile sx;
+  __shared__ LocalSnap ls;
   __shared__ int s_ok, s_active;
   unsigned int target = 0;
   const int nct = P.ntiles[0], nvt = P.ntiles[1], nlive = *P.nlive;
+  auto stamp = [&](int s, int k) { trace_stamp(P, s, k); };
+  if (threadIdx.x == 0) {
+    sm.acc = nullptr;
+    sm.cached = -1;
+    if (ONE) {
+      const int ii = P.live[0];
+      sm.inst = P.inst[ii];
+      sm.cached = ii;
+      const volatile InstCtrl* S = P.ctrl + ii;
+      ls.done = S->done;
+      ls.step = S->step;
+      ls.set = S->set;
+      ls.kcur = S->kcur;
+      ls.pending = S->pending;
+      ls.h = S->h_state;
+    }
+  }
+  __syncthreads();
+  if constexpr (XP) xp_setup<NT>(P, sx, xdyn, nct, nvt);
   for (int s = 0; s < nsteps; s++) {
-    if (threadIdx.x == 0) {
-      s_active = *(volatile int*)P.active;
-      sm.cached = -1;
-    }
-    __syncthreads();
-    if (s_active <= 0) break;  // grid-uniform: read after a barrier, written before one
-    for (int ti = blockIdx.x; ti < nct; ti += gridDim.x) {
-      load_tile<T, NT>(sm, P, P.ctiles, ti);
-      clause_tile<T, VEC, NT, XP>(P, sm, ti, xarea);
-    }
-    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
-    for (int ti = blockIdx.x; ti < nvt; ti += gridDim.x) {
-      load_tile<T, NT>(sm, P, P.vtiles, ti);
-      var_tile<T, G, SORTED, 0, NT, XP>(P, sm, nullptr, xarea, ti);
-    }
-    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
-    for (int k = blockIdx.x; k < nlive; k += gridDim.x) {
+    if constexpr (ONE) {
+      if (ls.done != 0) break;  // grid-uniform: every block applies the same decisions
+      if (threadIdx.x == 0) sm.acc = P.acc2 + (s & 1);
+    } else {
       if (threadIdx.x == 0) {
-        const int ii = P.live[k];
-        sm.inst = P.inst[ii];
-        sm.flag = (*(volatile int*)&P.ctrl[ii].done == 0);
-        sm.ti = ii;
+        s_active = *(volatile int*)P.active;
+        sm.cached = -1;
       }
       __syncthreads();
-      if (sm.flag) finalize_step<T, NT>(P, sm.inst, sm.ti, sm.red);
-      __syncthreads();
+      if (s_active <= 0) break;  // grid-uniform: read after a barrier, written before one
     }
+    stamp(s, 0);
+    if constexpr (XP) {
+      if (blockIdx.x < nct) {
+        load_tile_one<NT>(sm, ls, P.ctiles, blockIdx.x);
+        stamp(s, 1);
+        clause_tile_xp<NT>(P, sm, sx, xdyn, blockIdx.x, s);
+      }
+    } else {
+      for (int ti = blockIdx.x; ti < nct; ti += gridDim.x) {
+        if (ONE) load_tile_one<NT>(sm, ls, P.ctiles, ti);
+        else load_tile<T, NT>(sm, P, P.ctiles, ti);
+        stamp(s, 1);
+        stamp(s, 2);
+        clause_tile<T, VEC, NT>(P, sm, ti);
+      }
+    }
+    stamp(s, 3);
     if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    stamp(s, 4);
+    if (ONE && blockIdx.x == 0 && threadIdx.x == 0) {
+      StepAcc* z = P.acc2 + ((s + 1) & 1);
+      z->loc = 0;
+      z->vfail = 0;
+      z->kmax = 0;
+      z->energy = 0ull;
+    }
+    if constexpr (XP) {
+      if (blockIdx.x < nvt) {
+        load_tile_one<NT>(sm, ls, P.vtiles, blockIdx.x);
+        stamp(s, 5);
+        var_tile_xp<G, NT>(P, sm, sx, xdyn, s);
+      }
+    } else {
+      for (int ti = blockIdx.x; ti < nvt; ti += gridDim.x) {
+        if (ONE) load_tile_one<NT>(sm, ls, P.vtiles, ti);
+        else load_tile<T, NT>(sm, P, P.vtiles, ti);
+        stamp(s, 5);
+        stamp(s, 6);
+        var_tile<T, G, SORTED, 0, NT>(P, sm, nullptr);
+      }
+    }
+    stamp(s, 7);
+    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    stamp(s, 8);
+    if constexpr (ONE) {
+      if (threadIdx.x == 0) {
+        const volatile StepAcc* A = P.acc2 + (s & 1);
+        const int loc = A->loc, vfail = A->vfail, kmax = A->kmax;
+        if (blockIdx.x == 0) {
+          const double e = (double)A->energy * (1.0 / kEnergyUnitF32);
+          commit_step(P, sm.inst, P.live[0], loc, vfail, kmax, e);
+          __threadfence();
+        }
+        const StepDecision d = decide(loc, vfail, kmax, ls.step, sm.inst.max_steps);
+        ls.done = d.status;
+        ls.step += 1;
+        ls.set ^= 1;
+        ls.kcur = d.kacc;
+        ls.h = d.hs;
+        ls.pending = 1;
+      }
+      __syncthreads();
+      stamp(s, 9);
+    } else {
+      for (int k = blockIdx.x; k < nlive; k += gridDim.x) {
+        if (threadIdx.x == 0) {
+          const int ii = P.live[k];
+          sm.inst = P.inst[ii];
+          sm.flag = (*(volatile int*)&P.ctrl[ii].done == 0);
+          sm.ti = ii;
+        }
+        __syncthreads();
+        if (sm.flag) finalize_step<T, NT>(P, sm.inst, sm.ti, sm.red);
+        __syncthreads();
+      }
+      stamp(s, 9);
+      if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    }
   }
 }
 

@@ -1,6 +1,7 @@
 // Pack: device arrays, device-built CSR, tile tables and the CUDA-graph step loop.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -121,7 +122,10 @@ inline int blocks_for(int64_t work, int per = kThreads, int cap = 148 * 16) {
 constexpr int kMinClauseTile = 256;  // smallest clause tile (bounds the tile tables)
 constexpr int kMinVarTile = 32;      // smallest variable tile
 constexpr int kPersistThreads = 1024;  // block size of the cooperative step kernel
-constexpr int64_t kXposeBytes = 192 * 1024;  // shared memory of the staged transpose
+constexpr int kXpSmemMax = 200 * 1024;  // dynamic shared memory of the staged form, at most
+constexpr int kMiscInts = 32;            // misc_d_: 128 bytes
+constexpr int kMiscLaunch = 16;          // misc_d_ index of the per-launch area (byte 64)
+constexpr int kMiscAcc2 = 20;            // misc_d_ index of the StepAcc pair (byte 80)
 }  // namespace
 
 int64_t Pack::bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
@@ -146,8 +150,10 @@ Pack::~Pack() {
                   epart_,   inst_d_,    ctrl_d_,  ctiles_d_,   vtiles_d_,  ntiles_d_,
                   queue_d_, active_d_,  ring_d_,  ring_tail_d_, scan_tmp_, longv_d_,
                   stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_, order_d_,
-                  upos_,    xspos_,     xbidx_,   xgoff_,      xboff_};
+                  upos_,    trace_};
   for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (void* p : xbuf_)
     if (p) cudaFree(p);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
@@ -207,8 +213,10 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   DMM_CUDA(cudaMalloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&live_d_, I * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&order_d_, I * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&misc_d_, 8 * sizeof(int32_t)));
-  DMM_CUDA(cudaMemsetAsync(misc_d_, 0, 8 * sizeof(int32_t), stream_));
+  // [0] live formulas, [1] error flag, [3] k_inst queue; bytes 64..127: grid-barrier
+  // counter and the two step accumulators of the single-formula form (zeroed per launch)
+  DMM_CUDA(cudaMalloc(&misc_d_, kMiscInts * sizeof(int32_t)));
+  DMM_CUDA(cudaMemsetAsync(misc_d_, 0, kMiscInts * sizeof(int32_t), stream_));
   DMM_CUDA(cudaMemsetAsync(ctrl_d_, 0, I * sizeof(InstCtrl), stream_));
   DMM_CUDA(cudaMemsetAsync(ntiles_d_, 0, 4 * sizeof(int32_t), stream_));
   DMM_CUDA(cudaMemsetAsync(queue_d_, 0, 2 * sizeof(int32_t), stream_));
@@ -647,14 +655,24 @@ void Pack::fill_view(void* vv) const {
   v.ring_cap = caps_.insts;
   v.live = live_d_;
   v.nlive = misc_d_;
+  v.acc2 = reinterpret_cast<StepAcc*>(misc_d_ + kMiscAcc2);
   // tile paths: slot-major unless asked (measured faster there); the one-block-per-formula
   // kernel switches to variable-major by default in launch_inst
   v.upos = tun_.u_layout == 2 ? upos_ : nullptr;
-  v.xspos = xp_active_ ? xspos_ : nullptr;
-  v.xbidx = xbidx_;
-  v.xgoff = xgoff_;
-  v.xboff = xboff_;
-  v.xnct = xnct_;
+  v.xdlist = xp_active_ ? static_cast<const int32_t*>(xbuf_[kXpDlist]) : nullptr;
+  v.xdoff = static_cast<const int32_t*>(xbuf_[kXpDoff]);
+  v.xllit = static_cast<const int16_t*>(xbuf_[kXpLlit]);
+  v.xspos = static_cast<const uint16_t*>(xbuf_[kXpSpos]);
+  v.ux = static_cast<T*>(xbuf_[kXpUx]);
+  v.xubase = static_cast<const int32_t*>(xbuf_[kXpUbase]);
+  v.xboff = static_cast<const int32_t*>(xbuf_[kXpBoff]);
+  v.xsrc8 = static_cast<const int32_t*>(xbuf_[kXpSrc8]);
+  v.xdst = static_cast<const uint16_t*>(xbuf_[kXpDst]);
+  v.xsv_cap = xsv_cap_;
+  v.xbk_cap = xbk_cap_;
+  v.xtv_cap = xtv_cap_;
+  v.trace = trace_on_ ? trace_ : nullptr;
+  v.trace_steps = trace_on_ ? trace_steps_ : 0;
 }
 
 dmm_status Pack::enqueue_clause() {
@@ -724,98 +742,175 @@ static int occupancy_blocks(const void* fn, int threads, size_t smem = 0) {
   return std::max(1, b);
 }
 
-template <bool XP>
+// XP: staged form; ONE: single-formula form (both FP32 only)
+template <bool XP, bool ONE>
 static const void* persist_fn_x(dmm_precision prec, int G) {
-  if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads, XP>;
+  if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads>;
   switch (G) {
-    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, XP>;
-    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, XP>;
-    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads, XP>;
-    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads, XP>;
-    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads, XP>;
-    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads, XP>;
+    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, XP, ONE>;
+    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, XP, ONE>;
+    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads, XP, ONE>;
+    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads, XP, ONE>;
+    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads, XP, ONE>;
+    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads, XP, ONE>;
   }
 }
 
 const void* Pack::persist_fn() const {
-  return xp_active_ ? persist_fn_x<true>(prec_, tun_.var_group)
-                    : persist_fn_x<false>(prec_, tun_.var_group);
+  if (xp_active_) return persist_fn_x<true, true>(prec_, tun_.var_group);
+  if (one_active_) return persist_fn_x<false, true>(prec_, tun_.var_group);
+  return persist_fn_x<false, false>(prec_, tun_.var_group);
 }
 
-// Staged transpose of the contributions for a single formula on the cooperative path:
-// with one clause tile and one variable tile per block, block t stages its tile's
-// contributions in shared memory grouped by destination variable tile (ascending slot within
-// each group) and writes the area to u[3 t TC ..); variable tile b then copies the chunk of
-// every clause tile into its shared memory (ascending slot overall) and reduces through xbidx.
-// The per-variable summation order is unchanged.
+// Tables of the staged form (dmm_xpose.cuh) for formula idx with clause tiles of TC and
+// variable tiles of TV.  Leaves *ok false (and the plain tile code in use) when the
+// formula or its tiles do not fit the form's 16-bit indices or shared memory.
 dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   *ok = false;
   const InstDesc& I = inst_h_[idx];
-  if (!I.k3) return DMM_OK;
+  if (prec_ != DMM_FP32 || !I.k3) return DMM_OK;
   const int m = I.m, n = I.n, L = I.nslots;
   const int nct = (m + TC - 1) / TC, nvt = (n + TV - 1) / TV;
-  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_ || nct > kXpMaxChunks) return DMM_OK;
-  const int64_t cap = kXposeBytes / (int64_t)tsize_;
-  if (3 * (int64_t)TC > cap) return DMM_OK;
+  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_) return DMM_OK;
   std::vector<int32_t> lits(L), vsl(L);
   DMM_CUDA(cudaMemcpyAsync(lits.data(), lit_ + I.slot0, (size_t)L * 4, cudaMemcpyDeviceToHost, stream_));
   DMM_CUDA(cudaMemcpyAsync(vsl.data(), vslot_ + I.slot0, (size_t)L * 4, cudaMemcpyDeviceToHost, stream_));
   DMM_CUDA(cudaStreamSynchronize(stream_));
+  auto pad8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
   auto tile_of = [&](int s) { return (s / 3) / TC; };
-  auto bucket_of = [&](int s) { return (std::abs(lits[s]) - 1) / TV; };
-  std::vector<int32_t> cnt((size_t)nct * nvt, 0);
-  for (int s = 0; s < L; s++) cnt[(size_t)tile_of(s) * nvt + bucket_of(s)]++;
-  std::vector<int32_t> start((size_t)nct * nvt);
-  for (int t = 0; t < nct; t++) {
-    int32_t acc = 0;
+  auto vtile_of = [&](int s) { return (std::abs(lits[s]) - 1) / TV; };
+  // variable-major position of every slot; start of each variable tile's lists
+  std::vector<int32_t> vpos(L), jb(nvt + 1, 0);
+  for (int j = 0; j < L; j++) vpos[vsl[j]] = j;
+  {
+    std::vector<int32_t> per_tile(nvt, 0);
+    for (int s = 0; s < L; s++) per_tile[vtile_of(s)]++;
     for (int b = 0; b < nvt; b++) {
-      start[(size_t)t * nvt + b] = acc;
-      acc += cnt[(size_t)t * nvt + b];
+      if (per_tile[b] >= (int32_t)kXpPad) return DMM_OK;  // 16-bit bucket positions
+      jb[b + 1] = jb[b] + per_tile[b];
     }
   }
-  std::vector<int32_t> goff((size_t)nvt * nct), boff((size_t)nvt * (nct + 1));
+  std::vector<int32_t> cnt((size_t)nct * nvt, 0);
+  for (int s = 0; s < L; s++) cnt[(size_t)tile_of(s) * nvt + vtile_of(s)]++;
+  // staging area of clause tile t: chunk b at sb[t][b], sector-padded
+  std::vector<int32_t> sb((size_t)nct * nvt), ubase(nct + 1, 0);
+  int64_t st_max = 0;
+  for (int t = 0; t < nct; t++) {
+    int64_t acc = 0;
+    for (int b = 0; b < nvt; b++) {
+      sb[(size_t)t * nvt + b] = (int32_t)acc;
+      acc += pad8(cnt[(size_t)t * nvt + b]);
+    }
+    if (acc > 65535) return DMM_OK;  // 16-bit staging positions
+    st_max = std::max(st_max, acc);
+    if ((int64_t)ubase[t] + acc > INT32_MAX) return DMM_OK;
+    ubase[t + 1] = ubase[t] + (int32_t)acc;
+  }
+  // bucket of variable tile b: chunk of clause tile t at bt[b][t] (from boff[b])
+  std::vector<int32_t> bt((size_t)nvt * nct), boff(nvt + 1, 0);
+  int64_t bk_max = 0;
   for (int b = 0; b < nvt; b++) {
     int64_t acc = 0;
     for (int t = 0; t < nct; t++) {
-      goff[(size_t)b * nct + t] = 3 * t * TC + start[(size_t)t * nvt + b];
-      boff[(size_t)b * (nct + 1) + t] = (int32_t)acc;
-      acc += cnt[(size_t)t * nvt + b];
+      bt[(size_t)b * nct + t] = (int32_t)acc;
+      acc += pad8(cnt[(size_t)t * nvt + b]);
     }
-    if (acc > cap) return DMM_OK;  // bucket too large for shared memory
-    boff[(size_t)b * (nct + 1) + nct] = (int32_t)acc;
+    bk_max = std::max(bk_max, acc);
+    if ((int64_t)boff[b] + acc > INT32_MAX) return DMM_OK;
+    boff[b + 1] = boff[b] + (int32_t)acc;
   }
-  std::vector<uint16_t> spos(L), bidx(L);
+  // distinct variables of every clause tile (ascending) and the tile-local literals
+  std::vector<int32_t> dlist, doff(nct + 1, 0), where(n, -1);
+  std::vector<int16_t> llit(L);
+  int64_t sv_max = 0;
+  dlist.reserve(L);
+  for (int t = 0; t < nct; t++) {
+    const int s_lo = 3 * t * TC, s_hi = std::min(L, 3 * (t + 1) * TC);
+    const size_t d0 = dlist.size();
+    for (int s = s_lo; s < s_hi; s++) {
+      const int v = std::abs(lits[s]) - 1;
+      if (where[v] != t) {
+        where[v] = t;
+        dlist.push_back(v);
+      }
+    }
+    std::sort(dlist.begin() + d0, dlist.end());
+    const int64_t nd = (int64_t)(dlist.size() - d0);
+    if (nd > 32767) return DMM_OK;  // 16-bit signed local literals
+    sv_max = std::max(sv_max, nd);
+    doff[t + 1] = (int32_t)dlist.size();
+    for (size_t i = d0; i < dlist.size(); i++) where[dlist[i]] = -2 - (int32_t)(i - d0);
+    for (int s = s_lo; s < s_hi; s++) {
+      const int v = std::abs(lits[s]) - 1;
+      const int loc = -2 - where[v];
+      llit[s] = (int16_t)(lits[s] > 0 ? loc + 1 : -(loc + 1));
+    }
+    for (size_t i = d0; i < dlist.size(); i++) where[dlist[i]] = t;
+  }
+  // staging position of every slot (ascending slot within a chunk) and its bucket entry
+  std::vector<uint16_t> spos(L), dst(boff[nvt], kXpPad);
+  std::vector<int32_t> src8(boff[nvt] / 8);
   {
-    std::vector<int32_t> cur(start);
-    for (int s = 0; s < L; s++) spos[s] = (uint16_t)cur[(size_t)tile_of(s) * nvt + bucket_of(s)]++;
+    std::vector<int32_t> cur(sb);
+    for (int s = 0; s < L; s++) {
+      const int t = tile_of(s), b = vtile_of(s);
+      const int32_t q = cur[(size_t)t * nvt + b]++;
+      spos[s] = (uint16_t)q;
+      const int64_t p = (int64_t)boff[b] + bt[(size_t)b * nct + t] + (q - sb[(size_t)t * nvt + b]);
+      dst[p] = (uint16_t)(vpos[s] - jb[b]);
+    }
+    for (int b = 0; b < nvt; b++)
+      for (int t = 0; t < nct; t++) {
+        const int64_t g0 = ((int64_t)boff[b] + bt[(size_t)b * nct + t]) / 8;
+        const int64_t ng = pad8(cnt[(size_t)t * nvt + b]) / 8;
+        for (int64_t k = 0; k < ng; k++)
+          src8[g0 + k] = ubase[t] + sb[(size_t)t * nvt + b] + (int32_t)(8 * k);
+      }
   }
-  for (int j = 0; j < L; j++) {
-    const int s = vsl[j], t = tile_of(s), b = bucket_of(s);
-    bidx[j] = (uint16_t)(boff[(size_t)b * (nct + 1) + t] + (spos[s] - start[(size_t)t * nvt + b]));
-  }
-  auto grow = [&](void** p, int64_t* cap_now, int64_t bytes) -> dmm_status {
-    if (bytes <= *cap_now) return DMM_OK;
-    if (*p) DMM_CUDA(cudaFree(*p));
-    *p = nullptr;
-    DMM_CUDA(cudaMalloc(p, bytes));
-    *cap_now = bytes;
+  const int sv_cap = (int)std::max<int64_t>(sv_max, 1);
+  const int bk_cap = (int)std::max<int64_t>(std::max(st_max, bk_max), 8);
+  const int smem = xp_layout(sv_cap, bk_cap, TV).total;
+  if (smem > kXpSmemMax) return DMM_OK;
+  if (occupancy_blocks(persist_fn_x<true, true>(prec_, tun_.var_group), kPersistThreads, smem) * sms_ != grid_p_)
     return DMM_OK;
+  struct Up {
+    int which;
+    const void* src;
+    int64_t bytes;
   };
-  DMM_TRY(grow((void**)&xspos_, &xspos_cap_, (int64_t)caps_.slots * 2));
-  DMM_TRY(grow((void**)&xbidx_, &xbidx_cap_, (int64_t)caps_.slots * 2));
-  DMM_TRY(grow((void**)&xgoff_, &xgoff_cap_, (int64_t)goff.size() * 4));
-  DMM_TRY(grow((void**)&xboff_, &xboff_cap_, (int64_t)boff.size() * 4));
-  DMM_CUDA(cudaMemcpyAsync(xspos_ + I.slot0, spos.data(), (size_t)L * 2, cudaMemcpyHostToDevice, stream_));
-  DMM_CUDA(cudaMemcpyAsync(xbidx_ + I.slot0, bidx.data(), (size_t)L * 2, cudaMemcpyHostToDevice, stream_));
-  DMM_CUDA(cudaMemcpyAsync(xgoff_, goff.data(), goff.size() * 4, cudaMemcpyHostToDevice, stream_));
-  DMM_CUDA(cudaMemcpyAsync(xboff_, boff.data(), boff.size() * 4, cudaMemcpyHostToDevice, stream_));
+  const Up ups[] = {{kXpDlist, dlist.data(), (int64_t)dlist.size() * 4},
+                    {kXpDoff, doff.data(), (int64_t)doff.size() * 4},
+                    {kXpLlit, llit.data(), (int64_t)llit.size() * 2},
+                    {kXpSpos, spos.data(), (int64_t)spos.size() * 2},
+                    {kXpUx, nullptr, (int64_t)ubase[nct] * 4},
+                    {kXpUbase, ubase.data(), (int64_t)ubase.size() * 4},
+                    {kXpBoff, boff.data(), (int64_t)boff.size() * 4},
+                    {kXpSrc8, src8.data(), (int64_t)src8.size() * 4},
+                    {kXpDst, dst.data(), (int64_t)dst.size() * 2}};
+  for (const Up& u : ups) {
+    const int64_t bytes = std::max<int64_t>(u.bytes, 16);
+    if (bytes > xbuf_cap_[u.which]) {
+      if (xbuf_[u.which]) DMM_CUDA(cudaFree(xbuf_[u.which]));
+      xbuf_[u.which] = nullptr;
+      xbuf_cap_[u.which] = 0;
+      DMM_CUDA(cudaMalloc(&xbuf_[u.which], bytes));
+      xbuf_cap_[u.which] = bytes;
+    }
+    if (u.src && u.bytes > 0)
+      DMM_CUDA(cudaMemcpyAsync(xbuf_[u.which], u.src, u.bytes, cudaMemcpyHostToDevice, stream_));
+  }
   DMM_CUDA(cudaStreamSynchronize(stream_));
-  xnct_ = nct;
+  xsv_cap_ = sv_cap;
+  xbk_cap_ = bk_cap;
+  xtv_cap_ = TV;
+  xsmem_ = smem;
   *ok = true;
   return DMM_OK;
 }
 
 dmm_status Pack::commit_tiles() {
+  xp_active_ = false;
+  one_active_ = false;
   ctiles_h_.clear();
   vtiles_h_.clear();
   std::vector<int32_t> live_list;
@@ -896,14 +991,11 @@ dmm_status Pack::commit_tiles() {
     set_error("tile tables overflow");
     return DMM_ERR_BUDGET;
   }
-  // staged transpose: one formula, cooperative path, one tile of each kind per block
-  xp_active_ = false;
-  if (coop && live_list.size() == 1 && small_list.empty() && tun_.u_layout == 0 &&
-      tun_.clause_tile == 0 && tun_.var_tile == 0) {
-    const int32_t gp = occupancy_blocks(persist_fn_x<true>(prec_, tun_.var_group),
-                                        kPersistThreads, kXposeBytes) * sms_;
-    if (gp == grid_p_) DMM_TRY(prepare_xpose(live_list[0], TC, TV, &xp_active_));
-  }
+  // one FP32 formula on the cooperative path: two grid barriers per step; with the
+  // default layout and tiles, the staged form when it fits
+  one_active_ = coop && prec_ == DMM_FP32 && live_list.size() == 1 && small_list.empty();
+  if (one_active_ && tun_.u_layout == 0 && tun_.clause_tile == 0 && tun_.var_tile == 0)
+    DMM_TRY(prepare_xpose(live_list[0], TC, TV, &xp_active_));
   if (!ctiles_h_.empty())
     DMM_CUDA(cudaMemcpyAsync(ctiles_d_, ctiles_h_.data(), ctiles_h_.size() * sizeof(Tile),
                              cudaMemcpyHostToDevice, stream_));
@@ -939,11 +1031,14 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
     fill_view<float>(&vf);
     view = &vf;
   }
-  unsigned int* bar = reinterpret_cast<unsigned int*>(misc_d_ + 2);
+  static_assert(kMiscAcc2 * 4 + 2 * sizeof(StepAcc) <= kMiscInts * 4, "misc area");
+  unsigned int* bar = reinterpret_cast<unsigned int*>(misc_d_ + kMiscLaunch);
   int* err = misc_d_ + 1;
-  DMM_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned int), stream_));
+  DMM_CUDA(cudaMemsetAsync(bar, 0, (kMiscInts - kMiscLaunch) * sizeof(int32_t), stream_));
   void* args[] = {view, &nsteps, &bar, &err};
-  const size_t smem = xp_active_ ? (size_t)kXposeBytes : 0;
+  const size_t smem = xp_active_ ? (size_t)xsmem_ : 0;
+  if (smem)
+    DMM_CUDA(cudaFuncSetAttribute(persist_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(kPersistThreads), args,
                                        smem, stream_));
   return DMM_OK;
@@ -1070,6 +1165,66 @@ dmm_status Pack::time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double*
   }
   *ms = total;
   return check_error();
+}
+
+dmm_status Pack::trace_phases(int32_t nsteps, double* out) {
+  DMM_CUDA(cudaSetDevice(dev_));
+  if (tun_.launch_mode == 1 || n_small_ > 0 || nsteps <= 0) {
+    set_error("phase tracing needs the cooperative launch of tile-path formulas");
+    return DMM_ERR_STATE;
+  }
+  constexpr int K = kTraceK;
+  const int64_t need = (int64_t)nsteps * K * grid_p_;
+  if (need > trace_cap_) {
+    if (trace_) DMM_CUDA(cudaFree(trace_));
+    trace_ = nullptr;
+    DMM_CUDA(cudaMalloc(&trace_, need * sizeof(long long)));
+    trace_cap_ = need;
+  }
+  DMM_CUDA(cudaMemsetAsync(trace_, 0, need * sizeof(long long), stream_));
+  trace_on_ = true;
+  trace_steps_ = nsteps;
+  dmm_status st = launch_persist(nsteps);  // one launch: trace step s = launch step s
+  trace_on_ = false;
+  DMM_TRY(st);
+  std::vector<long long> h(need);
+  DMM_CUDA(cudaMemcpyAsync(h.data(), trace_, need * sizeof(long long), cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  DMM_TRY(check_error());
+  const int G = grid_p_;
+  auto at = [&](int64_t s, int k, int b) { return h[(s * K + k) * G + b]; };
+  double mean[K] = {}, mx[K] = {};
+  int used = 0;
+  // a step counts when every block stamped its start and the next step's start exists
+  for (int32_t s = 0; s + 1 < nsteps; s++) {
+    bool ok = true;
+    for (int b = 0; b < G && ok; b++) ok = at(s, 0, b) != 0 && at(s + 1, 0, b) != 0;
+    if (!ok) break;
+    double sm[K] = {}, smx[K] = {};
+    for (int b = 0; b < G; b++) {
+      long long pts[K + 1];
+      for (int k = 0; k < K; k++) {
+        const long long v = at(s, k, b);
+        pts[k] = v != 0 ? v : pts[k - 1];  // a block without a tile of the phase
+      }
+      pts[K] = at(s + 1, 0, b);
+      for (int k = 0; k < K; k++) {
+        const double d = (double)(pts[k + 1] - pts[k]);
+        sm[k] += d;
+        smx[k] = std::max(smx[k], d);
+      }
+    }
+    for (int k = 0; k < K; k++) {
+      mean[k] += sm[k] / G;
+      mx[k] += smx[k];
+    }
+    used++;
+  }
+  for (int k = 0; k < K; k++) {
+    out[2 * k] = used ? mean[k] / used / 1000.0 : 0.0;  // microseconds
+    out[2 * k + 1] = used ? mx[k] / used / 1000.0 : 0.0;
+  }
+  return DMM_OK;
 }
 
 dmm_status Pack::profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t) {

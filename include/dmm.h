@@ -224,6 +224,13 @@ dmm_status dmm_instance_time_steps(dmm_instance* inst, int32_t nsteps, double* m
  * with a cold L2; returns the summed device time of the steps (ms, flushes excluded). */
 dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
                                            int64_t flush_bytes, double* ms);
+/* Benchmark helper: one cooperative launch of nsteps steps with a device timer read by
+ * every block at 10 points of each step (start, clause tile loaded, voltages gathered,
+ * phase A done, past grid barrier 1, variable tile loaded, contributions gathered, phase B
+ * done, past barrier 2, step decision done).  out[20]: out[2k], out[2k+1] = mean and max
+ * over blocks of the microseconds from point k to point k+1 (point 10: the next step's
+ * start), averaged over steps.  DMM_ERR_STATE on the two-kernel launch form. */
+dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double* out);
 
 /* ---- right-hand side without device allocation ----------------------------------------- */
 /* No counterpart in the reference.  For callers that may not allocate device memory (a
