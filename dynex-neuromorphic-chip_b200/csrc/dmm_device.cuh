@@ -60,6 +60,7 @@ struct InstCtrl {
 struct StepAcc {
   int32_t loc, vfail, kmax, pad;
   unsigned long long energy;  // FP32 energy in units of 2^-25 (exact)
+  unsigned long long arrive;  // grid-barrier arrivals carrying trial indices (staged form)
 };
 
 struct Tile {
@@ -100,14 +101,15 @@ struct PackView {
   StepAcc* acc2;            // [2] step accumulators of the single-formula cooperative form
   // staged form (FP32, one formula of 3-literal clauses, cooperative launch, one clause
   // tile and one variable tile per block; xdlist null when off).  Clause tile t gathers
-  // the voltages of its distinct variables xdlist[xdoff[t] ..) into shared memory, reads
+  // the voltages of its distinct variables (ascending; xdlist from xdoff[2t], xdoff[2t+1]
+  // entries, 16-byte aligned) into shared memory, reads
   // them through the tile-local literals xllit (+-(1 + position in the list)), stages each
   // contribution at xspos in a shared area grouped by destination variable tile (chunks
   // padded to 8 entries) and writes the area to ux[xubase[t] ..).  Variable tile b reads
   // bucket positions [xboff[b], xboff[b + 1]) (ux index of every 8 positions in xsrc8)
   // and scatters them to their variable-major positions xdst in shared memory.
   const int32_t* xdlist;
-  const int32_t* xdoff;     // [clause tiles + 1]
+  const int32_t* xdoff;     // [2 * clause tiles]: start, count
   const int16_t* xllit;     // per slot of the formula
   const uint16_t* xspos;    // per slot of the formula
   T* ux;

@@ -463,12 +463,6 @@ __global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restr
   }
 }
 
-}  // namespace dmm
-
-#include "dmm_xpose.cuh"
-
-namespace dmm {
-
 // ---- persistent form -------------------------------------------------------------------------
 
 // Grid barrier for a cooperative launch: a monotonic arrival counter (zeroed before the
@@ -536,14 +530,10 @@ __device__ __forceinline__ void load_tile_one(TileSmem<NT>& sm, const LocalSnap&
 // once barrier 1 of step s has passed, after every block has read it in step s-1); after
 // barrier 2 every block reads them and applies the step decision to its own copy of the
 // control state, and block 0 writes the control state for the host.
-// XP: the staged form (implies ONE; clause tile and variable tile b belong to block b).
-template <class T, int G, bool SORTED, bool VEC, int NT, bool XP = false, bool ONE = false>
+template <class T, int G, bool SORTED, bool VEC, int NT, bool ONE = false>
 __global__ void __launch_bounds__(NT, 1)
     k_persist(PackView<T> P, int nsteps, unsigned int* bar, int* err) {
-  static_assert(!XP || ONE, "the staged form runs with one formula");
   __shared__ TileSmem<NT> sm;
-  extern __shared__ __align__(16) unsigned char xdyn[];  // staged form only
-  __shared__ XpTile sx;
   __shared__ LocalSnap ls;
   __shared__ int s_ok, s_active;
   unsigned int target = 0;
@@ -566,7 +556,6 @@ __global__ void __launch_bounds__(NT, 1)
     }
   }
   __syncthreads();
-  if constexpr (XP) xp_setup<NT>(P, sx, xdyn, nct, nvt);
   for (int s = 0; s < nsteps; s++) {
     if constexpr (ONE) {
       if (ls.done != 0) break;  // grid-uniform: every block applies the same decisions
@@ -580,20 +569,12 @@ __global__ void __launch_bounds__(NT, 1)
       if (s_active <= 0) break;  // grid-uniform: read after a barrier, written before one
     }
     stamp(s, 0);
-    if constexpr (XP) {
-      if (blockIdx.x < nct) {
-        load_tile_one<NT>(sm, ls, P.ctiles, blockIdx.x);
-        stamp(s, 1);
-        clause_tile_xp<NT>(P, sm, sx, xdyn, blockIdx.x, s);
-      }
-    } else {
-      for (int ti = blockIdx.x; ti < nct; ti += gridDim.x) {
-        if (ONE) load_tile_one<NT>(sm, ls, P.ctiles, ti);
-        else load_tile<T, NT>(sm, P, P.ctiles, ti);
-        stamp(s, 1);
-        stamp(s, 2);
-        clause_tile<T, VEC, NT>(P, sm, ti);
-      }
+    for (int ti = blockIdx.x; ti < nct; ti += gridDim.x) {
+      if (ONE) load_tile_one<NT>(sm, ls, P.ctiles, ti);
+      else load_tile<T, NT>(sm, P, P.ctiles, ti);
+      stamp(s, 1);
+      stamp(s, 2);
+      clause_tile<T, VEC, NT>(P, sm, ti);
     }
     stamp(s, 3);
     if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
@@ -604,21 +585,14 @@ __global__ void __launch_bounds__(NT, 1)
       z->vfail = 0;
       z->kmax = 0;
       z->energy = 0ull;
+      z->arrive = 0ull;
     }
-    if constexpr (XP) {
-      if (blockIdx.x < nvt) {
-        load_tile_one<NT>(sm, ls, P.vtiles, blockIdx.x);
-        stamp(s, 5);
-        var_tile_xp<G, NT>(P, sm, sx, xdyn, s);
-      }
-    } else {
-      for (int ti = blockIdx.x; ti < nvt; ti += gridDim.x) {
-        if (ONE) load_tile_one<NT>(sm, ls, P.vtiles, ti);
-        else load_tile<T, NT>(sm, P, P.vtiles, ti);
-        stamp(s, 5);
-        stamp(s, 6);
-        var_tile<T, G, SORTED, 0, NT>(P, sm, nullptr);
-      }
+    for (int ti = blockIdx.x; ti < nvt; ti += gridDim.x) {
+      if (ONE) load_tile_one<NT>(sm, ls, P.vtiles, ti);
+      else load_tile<T, NT>(sm, P, P.vtiles, ti);
+      stamp(s, 5);
+      stamp(s, 6);
+      var_tile<T, G, SORTED, 0, NT>(P, sm, nullptr);
     }
     stamp(s, 7);
     if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
@@ -661,3 +635,5 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 }  // namespace dmm
+
+#include "dmm_xpose.cuh"

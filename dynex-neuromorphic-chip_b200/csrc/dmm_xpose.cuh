@@ -1,43 +1,51 @@
-// Staged form of phases A and B (FP32, one formula of 3-literal clauses, cooperative launch
-// with one clause tile and one variable tile per block).
+// Staged form of the integration step: FP32, one formula of 3-literal clauses, one
+// cooperative launch with one clause tile and one variable tile per block.
 //
 // The plain tile code issues one L2 request per literal occurrence in each phase (phase A
-// gathers V[|l|-1] per literal, phase B gathers u through the variable->slot list), and each
-// request sits behind a dependent global load.  The staged form moves both gathers into
-// shared memory:
+// gathers V[|l|-1] per literal, phase B gathers u through the variable->slot list), each
+// behind a dependent global load.  The staged form moves both gathers into shared memory:
 //
-//   A  the voltages of the clause tile's distinct variables are gathered once, in ascending
-//      variable order (neighbouring lanes share 32-byte sectors), into shared memory; the
-//      clauses read them through 16-bit tile-local literals.  Each contribution is written
-//      to a shared staging area grouped by destination variable tile (one chunk per
-//      variable tile, padded to 8 entries = one sector) and the area is written to global
-//      memory with 16-byte stores.
-//   B  a variable tile copies its chunk from every clause tile (coalesced: chunks are
-//      contiguous and sector-aligned) and scatters the values into shared memory at their
-//      variable-major positions, then reduces each variable from there.
+//   A  the clause tile's distinct variables (ascending, kept in shared memory for the whole
+//      launch) have their voltages gathered by asynchronous copies into shared memory;
+//      the clauses read them through 16-bit tile-local literals.  Each contribution is
+//      written to a shared staging area grouped by destination variable tile (one chunk
+//      per variable tile, padded to 8 entries = one sector) and the area is written to
+//      global memory with 16-byte stores.
+//   B  a variable tile copies its chunk of every clause tile (contiguous, sector-aligned)
+//      with 4-byte asynchronous copies straight to each value's variable-major position
+//      in shared memory, then reduces each variable from there.
+//
+// Grid barriers are split (arrive ... wait) so that loads that do not depend on the other
+// blocks (the destination positions and voltages of phase B) are in flight during the wait.
+// Barrier 2 carries the step decision: a block arrives by adding 1 << (12 k) to the step's
+// arrival word, k = the largest trial index of its variables, so that the word that ends
+// the wait also holds the step's largest trial index.  The step's unsatisfied count and
+// strict-sign failures (complete at barrier 1) are read during phase B.  Every block applies
+// the decision to its own copy of the control state; block 0 writes it for the host.
 //
 // Every clause value and every per-variable sum is computed from the same operands in the
 // same order as the plain tile code, so results are identical to it.
 #pragma once
 
-#include "dmm_kernels.cuh"
-
 namespace dmm {
 
-constexpr int kXpUnroll = 8;            // independent loads per thread in the staged gathers
-constexpr uint16_t kXpPad = 0xFFFF;     // xdst of a padding entry
+constexpr uint16_t kXpPad = 0xFFFF;  // xdst of a padding entry
+constexpr int kXpPairs = 10;         // destination pairs per thread loaded across barrier 1
+constexpr int kArriveBits = 12;      // width of one trial's arrival count (> grid size)
+constexpr int kPollSleepNs = 64;     // back-off between polls of a barrier word
 
 __host__ __device__ constexpr int xp_align16(int bytes) { return (bytes + 15) & ~15; }
 
 // Dynamic shared-memory layout of the staged form (byte offsets).
 struct XpLayout {
-  int sv, bk, src8, vend, cur, unit, total;
+  int sd, sv, bk, src8, vend, cur, unit, total;
 };
 
 __host__ __device__ inline XpLayout xp_layout(int sv_cap, int bk_cap, int tv_cap) {
   XpLayout L;
   int o = 0;
-  L.sv = o;   o += xp_align16(4 * sv_cap);        // voltages of the clause tile's variables
+  L.sd = o;                                       // (unused: the list is read per step)
+  L.sv = o;   o += xp_align16(4 * sv_cap);        // the tile's variables, then their voltages
   L.bk = o;   o += xp_align16(4 * bk_cap);        // staging area (A) / bucket (B)
   L.src8 = o; o += xp_align16(4 * (bk_cap / 8));  // ux index of every 8 bucket positions
   L.vend = o; o += xp_align16(4 * (tv_cap + 1));  // tile-local CSR ends of the variable tile
@@ -47,290 +55,437 @@ __host__ __device__ inline XpLayout xp_layout(int sv_cap, int bk_cap, int tv_cap
   return L;
 }
 
-// Per-block ranges of the staged form (constant for a launch).
-struct XpTile {
-  int dbeg, dcnt;   // distinct variables of the clause tile: xdlist[dbeg, dbeg + dcnt)
-  int ubase, ulen;  // staging area of the clause tile: ux[ubase, ubase + ulen)
-  int bbeg, blen;   // bucket of the variable tile: positions [bbeg, bbeg + blen)
+// Asynchronous global->shared copies (completed by cp_async_wait_all + a block barrier).
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Entry k (0..11) of twelve 16-bit values held in three 8-byte words; k must fold to a
+// constant (unrolled loops), so the words stay in registers.
+__device__ __forceinline__ int i16_at(const int2 (&w)[3], int k) {
+  const int word = (k & 2) ? w[k >> 2].y : w[k >> 2].x;
+  return (k & 1) ? (word >> 16) : (int)(short)(word & 0xffff);
+}
+__device__ __forceinline__ int u16_at(const uint2 (&w)[3], int k) {
+  const unsigned word = (k & 2) ? w[k >> 2].y : w[k >> 2].x;
+  return (int)((k & 1) ? (word >> 16) : (word & 0xffffu));
+}
+__device__ __forceinline__ float f4_at(const float4& v, int i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
+// The block's copy of the control state of the formula.
+struct StagedCtrl {
+  int done, step, set, kcur, pending, best_loc;
+  double h, t, best_t;
 };
 
-// Loads the launch-constant tables of block b's variable tile into shared memory.
-template <int NT>
-__device__ void xp_setup(const PackView<float>& P, XpTile& sx, unsigned char* dyn, int nct,
-                         int nvt) {
-  const XpLayout L = xp_layout(P.xsv_cap, P.xbk_cap, P.xtv_cap);
-  const int b = blockIdx.x;
-  if (threadIdx.x == 0) {
-    XpTile x = {0, 0, 0, 0, 0, 0};
-    if (b < nct) {
-      x.dbeg = __ldg(P.xdoff + b);
-      x.dcnt = __ldg(P.xdoff + b + 1) - x.dbeg;
-      x.ubase = __ldg(P.xubase + b);
-      x.ulen = __ldg(P.xubase + b + 1) - x.ubase;
-    }
-    if (b < nvt) {
-      x.bbeg = __ldg(P.xboff + b);
-      x.blen = __ldg(P.xboff + b + 1) - x.bbeg;
-    }
-    sx = x;
+// Operands of one group of 4 clauses.
+struct Group4 {
+  int2 lw[3];   // 12 tile-local literals
+  uint2 qw[3];  // 12 staging positions
+  float4 xs, xl, cp, al;
+};
+
+__device__ __forceinline__ void load_words4(Group4& q, const int16_t* ll, const uint16_t* sp,
+                                            int g) {
+  const int2* L2 = reinterpret_cast<const int2*>(ll + 3 * g);
+  const uint2* Q2 = reinterpret_cast<const uint2*>(sp + 3 * g);
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    q.lw[r] = __ldg(L2 + r);
+    q.qw[r] = __ldg(Q2 + r);
   }
-  __syncthreads();
-  if (b < nvt) {
-    const Tile vt = P.vtiles[b];
-    const int64_t var0 = P.inst[vt.inst].var0;
-    const int32_t* __restrict__ vend = P.vend + var0;
-    const int jb = vt.begin > 0 ? __ldg(vend + vt.begin - 1) : 0;
-    int32_t* s_src8 = reinterpret_cast<int32_t*>(dyn + L.src8);
-    int32_t* s_vend = reinterpret_cast<int32_t*>(dyn + L.vend);
-    int8_t* s_unit = reinterpret_cast<int8_t*>(dyn + L.unit);
-    const int32_t* __restrict__ src8 = P.xsrc8 + sx.bbeg / 8;
-    for (int g = threadIdx.x; g < sx.blen / 8; g += NT) s_src8[g] = __ldg(src8 + g);
-    for (int i = threadIdx.x; i <= vt.count; i += NT)
-      s_vend[i] = i == 0 ? 0 : __ldg(vend + vt.begin + i - 1) - jb;
-    for (int i = threadIdx.x; i < vt.count; i += NT) s_unit[i] = P.unit[var0 + vt.begin + i];
-  }
-  __syncthreads();
 }
 
-__device__ __forceinline__ void unpack_i16x4(int2 w, int* out) {
-  out[0] = (int)(short)(w.x & 0xffff);
-  out[1] = w.x >> 16;
-  out[2] = (int)(short)(w.y & 0xffff);
-  out[3] = w.y >> 16;
+__device__ __forceinline__ void load_state4(Group4& q, const float* Xs, const float* Xl,
+                                            const float* Cp, const float* acm, float alpha,
+                                            bool pending, int g) {
+  q.xs = *reinterpret_cast<const float4*>(Xs + g);
+  q.xl = *reinterpret_cast<const float4*>(Xl + g);
+  q.cp = pending ? *reinterpret_cast<const float4*>(Cp + g) : make_float4(0.f, 0.f, 0.f, 0.f);
+  q.al = acm ? *reinterpret_cast<const float4*>(acm + g) : make_float4(alpha, alpha, alpha, alpha);
 }
 
-__device__ __forceinline__ void unpack_u16x4(uint2 w, int* out) {
-  out[0] = (int)(w.x & 0xffffu);
-  out[1] = (int)(w.x >> 16);
-  out[2] = (int)(w.y & 0xffffu);
-  out[3] = (int)(w.y >> 16);
-}
-
-// ---- phase A, staged -------------------------------------------------------------------------
-template <int NT>
-__device__ void clause_tile_xp(const PackView<float>& P, TileSmem<NT>& sm, const XpTile& X,
-                               unsigned char* dyn, int ti, int step) {
-  if (sm.snap.done != 0) return;  // block-uniform
+template <int G, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_staged(PackView<float> P, int nsteps, unsigned int* bar, int* err) {
   using T = float;
+  extern __shared__ __align__(16) unsigned char staged_smem[];
+  __shared__ InstDesc I;
+  __shared__ StagedCtrl lc;
+  __shared__ Tile ctile, vtile;
+  __shared__ int dbeg, dcnt, ubase, ulen, bbeg, blen;
+  __shared__ double red[NT / 32];
+  __shared__ int cnt[2][NT / 32];
+  __shared__ int s_ok, s_loc, s_vfail;
+  __shared__ unsigned long long s_energy;
   const XpLayout LY = xp_layout(P.xsv_cap, P.xbk_cap, P.xtv_cap);
-  T* sV = reinterpret_cast<T*>(dyn + LY.sv);
-  T* stage = reinterpret_cast<T*>(dyn + LY.bk);
-  const InstDesc& I = sm.inst;
-  const ClauseConsts<T> kc = make_consts<T>(I, sm.snap.h);
-  const bool pending = sm.snap.pending != 0;
-  const T* V = P.cand + (int64_t)(sm.snap.set * kTrials + sm.snap.kcur) * P.var_cap + I.var0;
-  {
-    const int32_t* __restrict__ dl = P.xdlist + X.dbeg;
-    const int nd = X.dcnt;
-    for (int i0 = threadIdx.x; i0 < nd; i0 += kXpUnroll * NT) {
-      T val[kXpUnroll];
-#pragma unroll
-      for (int k = 0; k < kXpUnroll; k++) {
-        const int i = i0 + k * NT;
-        if (i < nd) val[k] = V[__ldg(dl + i)];
-      }
-#pragma unroll
-      for (int k = 0; k < kXpUnroll; k++) {
-        const int i = i0 + k * NT;
-        if (i < nd) sV[i] = val[k];
-      }
+  T* sV = reinterpret_cast<T*>(staged_smem + LY.sv);
+  T* stage = reinterpret_cast<T*>(staged_smem + LY.bk);  // phase A
+  T* bucket = stage;                             // phase B
+  int* s_src8 = reinterpret_cast<int*>(staged_smem + LY.src8);
+  int* s_vend = reinterpret_cast<int*>(staged_smem + LY.vend);
+  T* s_cur = reinterpret_cast<T*>(staged_smem + LY.cur);
+  int8_t* s_unit = reinterpret_cast<int8_t*>(staged_smem + LY.unit);
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const int nct = P.ntiles[0], nvt = P.ntiles[1];
+  const bool has_c = b < nct, has_v = b < nvt;
+  const int ii = P.live[0];
+
+  // ---- launch setup: description, control state, ranges, launch-constant tables
+  if (tid == 0) {
+    I = P.inst[ii];
+    const volatile InstCtrl* S = P.ctrl + ii;
+    lc.done = S->done;
+    lc.step = S->step;
+    lc.set = S->set;
+    lc.kcur = S->kcur;
+    lc.pending = S->pending;
+    lc.best_loc = S->best_loc;
+    lc.h = S->h_state;
+    lc.t = S->t;
+    lc.best_t = S->best_t;
+    dbeg = dcnt = ubase = ulen = bbeg = blen = 0;
+    if (has_c) {
+      ctile = P.ctiles[b];
+      dbeg = __ldg(P.xdoff + 2 * b);
+      dcnt = __ldg(P.xdoff + 2 * b + 1);
+      ubase = __ldg(P.xubase + b);
+      ulen = __ldg(P.xubase + b + 1) - ubase;
+    }
+    if (has_v) {
+      vtile = P.vtiles[b];
+      bbeg = __ldg(P.xboff + b);
+      blen = __ldg(P.xboff + b + 1) - bbeg;
     }
   }
   __syncthreads();
-  trace_stamp(P, step, 2);
-  T* __restrict__ Xs = P.Xs + I.cls0;
-  T* __restrict__ Xl = P.Xl + I.cls0;
-  T* __restrict__ Cp = P.Cp + I.cls0;
-  const T* __restrict__ acm = I.has_alpha_cm ? P.alpha_cm + I.cls0 : nullptr;
-  const int16_t* __restrict__ ll = P.xllit;
-  const uint16_t* __restrict__ sp = P.xspos;
-  const int c_begin = sm.tile.begin, c_end = sm.tile.begin + sm.tile.count;
-  int unsat = 0, vfail = 0;
-  double e = 0.0;
-  for (int g = c_begin + 4 * threadIdx.x; g < c_end; g += 4 * NT) {
-    const int nc = min(4, c_end - g);
-    int L[12], Q[12];
-    T xs[4], xl[4], cp[4], al[4];
-    if (nc == 4) {
-      const int2* L2 = reinterpret_cast<const int2*>(ll + 3 * g);
-      const uint2* Q2 = reinterpret_cast<const uint2*>(sp + 3 * g);
-#pragma unroll
-      for (int r = 0; r < 3; r++) {
-        unpack_i16x4(__ldg(L2 + r), L + 4 * r);
-        unpack_u16x4(__ldg(Q2 + r), Q + 4 * r);
-      }
-      const float4 xs4 = *reinterpret_cast<const float4*>(Xs + g);
-      const float4 xl4 = *reinterpret_cast<const float4*>(Xl + g);
-      float4 cp4 = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (pending) cp4 = *reinterpret_cast<const float4*>(Cp + g);
-      float4 al4 = make_float4(kc.alpha, kc.alpha, kc.alpha, kc.alpha);
-      if (acm) al4 = *reinterpret_cast<const float4*>(acm + g);
-      xs[0] = xs4.x; xs[1] = xs4.y; xs[2] = xs4.z; xs[3] = xs4.w;
-      xl[0] = xl4.x; xl[1] = xl4.y; xl[2] = xl4.z; xl[3] = xl4.w;
-      cp[0] = cp4.x; cp[1] = cp4.y; cp[2] = cp4.z; cp[3] = cp4.w;
-      al[0] = al4.x; al[1] = al4.y; al[2] = al4.z; al[3] = al4.w;
-    } else {
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        xs[i] = xl[i] = cp[i] = T(0);
-        al[i] = kc.alpha;
-#pragma unroll
-        for (int j = 0; j < 3; j++) L[3 * i + j] = Q[3 * i + j] = 0;
-        if (i < nc) {
-          const int c = g + i;
-#pragma unroll
-          for (int j = 0; j < 3; j++) {
-            L[3 * i + j] = __ldg(ll + 3 * c + j);
-            Q[3 * i + j] = __ldg(sp + 3 * c + j);
-          }
-          xs[i] = Xs[c];
-          xl[i] = Xl[c];
-          if (pending) cp[i] = Cp[c];
-          if (acm) al[i] = acm[c];
-        }
-      }
-    }
-    T cc[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      cc[i] = T(0);
-      if (i < nc) {
-        if (pending) advance_memory(xs[i], xl[i], cp[i], al[i], kc);
+  if (has_v) {
+    const int32_t* vend = P.vend + I.var0;
+    const int jb = vtile.begin > 0 ? __ldg(vend + vtile.begin - 1) : 0;
+    for (int g = tid; g < blen / 8; g += NT) s_src8[g] = __ldg(P.xsrc8 + bbeg / 8 + g);
+    for (int i = tid; i <= vtile.count; i += NT)
+      s_vend[i] = i == 0 ? 0 : __ldg(vend + vtile.begin + i - 1) - jb;
+    for (int i = tid; i < vtile.count; i += NT) s_unit[i] = P.unit[I.var0 + vtile.begin + i];
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  unsigned int target = 0;
+
+  for (int s = 0; s < nsteps; s++) {
+    if (lc.done != 0) break;  // grid-uniform: every block applies the same decisions
+    trace_stamp(P, s, 0);
+    StepAcc* acc = P.acc2 + (s & 1);
+    const int set = lc.set, kcur = lc.kcur;
+    const bool pending = lc.pending != 0;
+    const ClauseConsts<T> kc = make_consts<T>(I, lc.h);
+    const T* V = P.cand + (int64_t)(set * kTrials + kcur) * P.var_cap + I.var0;
+    trace_stamp(P, s, 1);
+
+    // ---- phase A
+    if (has_c) {
+      T* __restrict__ Xs = P.Xs + I.cls0;
+      T* __restrict__ Xl = P.Xl + I.cls0;
+      T* __restrict__ Cp = P.Cp + I.cls0;
+      const T* __restrict__ acm = I.has_alpha_cm ? P.alpha_cm + I.cls0 : nullptr;
+      const int16_t* __restrict__ ll = P.xllit;
+      const uint16_t* __restrict__ sp = P.xspos;
+      // the tile's variable list (padded to 4 entries), then each entry replaced in place
+      // by its voltage: two rounds of asynchronous copies with every load in flight
+      int* sVi = reinterpret_cast<int*>(sV);
+      for (int q = tid; 4 * q < dcnt; q += NT) cp_async16(sVi + 4 * q, P.xdlist + dbeg + 4 * q);
+      cp_async_wait_all();
+      __syncthreads();
+      for (int i = tid; i < dcnt; i += NT) cp_async4(sV + i, V + sVi[i]);
+      const int c_begin = ctile.begin, c_end = ctile.begin + ctile.count;
+      const int g0 = c_begin + 4 * tid;
+      cp_async_wait_all();
+      __syncthreads();
+      trace_stamp(P, s, 2);
+      int unsat = 0, vfail = 0;
+      double e = 0.0;
+      auto one = [&](int l0, int l1, int l2, int p0, int p1, int p2, T& xs, T& xl, T cp,
+                     T al) -> T {
+        if (pending) advance_memory(xs, xl, cp, al, kc);
         bool ss;
         T u0, u1, u2;
-        const T C = clause3(L[3 * i], L[3 * i + 1], L[3 * i + 2], sV[abs(L[3 * i]) - 1],
-                            sV[abs(L[3 * i + 1]) - 1], sV[abs(L[3 * i + 2]) - 1], xs[i], xl[i],
-                            kc, u0, u1, u2, ss);
-        stage[Q[3 * i]] = u0;
-        stage[Q[3 * i + 1]] = u1;
-        stage[Q[3 * i + 2]] = u2;
-        cc[i] = C;
+        const T C = clause3(l0, l1, l2, sV[abs(l0) - 1], sV[abs(l1) - 1], sV[abs(l2) - 1], xs,
+                            xl, kc, u0, u1, u2, ss);
+        stage[p0] = u0;
+        stage[p1] = u1;
+        stage[p2] = u2;
         unsat += !(C < T(0.5));
         vfail += !ss;
         e += (double)C * kEnergyUnitF32;
-      }
-    }
-    if (nc == 4) {
-      *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
-      *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
-      *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
-    } else {
-      for (int i = 0; i < nc; i++) {
-        Xs[g + i] = xs[i];
-        Xl[g + i] = xl[i];
-        Cp[g + i] = cc[i];
-      }
-    }
-  }
-  const int w = threadIdx.x >> 5;
-  unsat = warp_sum_i(unsat);
-  vfail = warp_sum_i(vfail);
-  if ((threadIdx.x & 31) == 0) {
-    sm.cnt[0][w] = unsat;
-    sm.cnt[1][w] = vfail;
-  }
-  const double et = block_sum<NT>(e, sm.red);  // also completes the staging area
-  {
-    float4* __restrict__ dst = reinterpret_cast<float4*>(P.ux + X.ubase);
-    const float4* src = reinterpret_cast<const float4*>(stage);
-    for (int i = threadIdx.x; i < X.ulen / 4; i += NT) dst[i] = src[i];
-  }
-  if (threadIdx.x == 0) {
-    int tu = 0, tv = 0;
+        return C;
+      };
+      auto group = [&](const Group4& q, int g) {
+        T xs[4] = {q.xs.x, q.xs.y, q.xs.z, q.xs.w};
+        T xl[4] = {q.xl.x, q.xl.y, q.xl.z, q.xl.w};
+        T cc[4];
 #pragma unroll
-    for (int i = 0; i < NT / 32; i++) {
-      tu += sm.cnt[0][i];
-      tv += sm.cnt[1][i];
-    }
-    add_clause_counts(P, sm, ti, tu, tv, et);
-  }
-  __syncthreads();
-}
-
-// ---- phase B, staged -------------------------------------------------------------------------
-template <int G, int NT>
-__device__ void var_tile_xp(const PackView<float>& P, TileSmem<NT>& sm, const XpTile& X,
-                            unsigned char* dyn, int step) {
-  if (sm.snap.done != 0) return;  // block-uniform
-  using T = float;
-  const XpLayout LY = xp_layout(P.xsv_cap, P.xbk_cap, P.xtv_cap);
-  T* bucket = reinterpret_cast<T*>(dyn + LY.bk);
-  const int32_t* s_src8 = reinterpret_cast<const int32_t*>(dyn + LY.src8);
-  const int32_t* s_vend = reinterpret_cast<const int32_t*>(dyn + LY.vend);
-  T* s_cur = reinterpret_cast<T*>(dyn + LY.cur);
-  const int8_t* s_unit = reinterpret_cast<const int8_t*>(dyn + LY.unit);
-  const InstDesc& I = sm.inst;
-  const T* cur = P.cand + (int64_t)(sm.snap.set * kTrials + sm.snap.kcur) * P.var_cap + I.var0;
-  T* __restrict__ nxt = P.cand + (int64_t)((sm.snap.set ^ 1) * kTrials) * P.var_cap + I.var0;
-  const int v0 = sm.tile.begin, nv = sm.tile.count;
-  // the tile's voltages and its chunk of every clause tile, with all loads in flight
-  T cv = T(0);
-  if (threadIdx.x < nv) cv = cur[v0 + threadIdx.x];
-  {
-    const uint16_t* __restrict__ xd = P.xdst + X.bbeg;
-    const T* ux = P.ux;
-    const int nb = X.blen;
-    for (int p0 = threadIdx.x; p0 < nb; p0 += kXpUnroll * NT) {
-      T val[kXpUnroll];
-      int d[kXpUnroll];
-#pragma unroll
-      for (int k = 0; k < kXpUnroll; k++) {
-        const int p = p0 + k * NT;
-        d[k] = kXpPad;
-        if (p < nb) {
-          val[k] = ux[s_src8[p >> 3] + (p & 7)];
-          d[k] = __ldg(xd + p);
+        for (int i = 0; i < 4; i++)
+          cc[i] = one(i16_at(q.lw, 3 * i), i16_at(q.lw, 3 * i + 1), i16_at(q.lw, 3 * i + 2),
+                      u16_at(q.qw, 3 * i), u16_at(q.qw, 3 * i + 1), u16_at(q.qw, 3 * i + 2), xs[i],
+                      xl[i], f4_at(q.cp, i), f4_at(q.al, i));
+        *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
+        *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
+        *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+      };
+      for (int g = g0; g < c_end; g += 4 * NT) {
+        if (g + 4 <= c_end) {
+          Group4 q;
+          load_words4(q, ll, sp, g);
+          load_state4(q, Xs, Xl, Cp, acm, kc.alpha, pending, g);
+          group(q, g);
+        } else {
+          for (int c = g; c < c_end; c++) {
+            T xs = Xs[c], xl = Xl[c];
+            const T cp = pending ? Cp[c] : T(0);
+            const T al = acm ? acm[c] : kc.alpha;
+            Cp[c] = one(__ldg(ll + 3 * c), __ldg(ll + 3 * c + 1), __ldg(ll + 3 * c + 2),
+                        __ldg(sp + 3 * c), __ldg(sp + 3 * c + 1), __ldg(sp + 3 * c + 2), xs, xl,
+                        cp, al);
+            Xs[c] = xs;
+            Xl[c] = xl;
+          }
         }
       }
-#pragma unroll
-      for (int k = 0; k < kXpUnroll; k++)
-        if (d[k] != kXpPad) bucket[d[k]] = val[k];
-    }
-  }
-  if (threadIdx.x < nv) s_cur[threadIdx.x] = cv;
-  for (int i = threadIdx.x + NT; i < nv; i += NT) s_cur[i] = cur[v0 + i];
-  __syncthreads();
-  trace_stamp(P, step, 6);
-  constexpr int VPP = NT / G;
-  const int grp = threadIdx.x / G, lane = threadIdx.x % G;
-  int kmax = 0;
-  for (int vb = 0; vb < nv; vb += VPP) {
-    const int i = vb + grp;
-    const bool valid = i < nv;
-    int s0 = 0, s1 = 0;
-    if (valid) {
-      s0 = s_vend[i];
-      s1 = s_vend[i + 1];
-    }
-    const T dv = tree_sum<T, G, true, int32_t>(bucket + s0, nullptr, s1 - s0, lane);
-    if (valid && lane == 0) {
-      const T V = s_cur[i];
-      const int8_t un = s_unit[i];
-      const int v = v0 + i;
-      int kv = kTrials;
-#pragma unroll
-      for (int k = 0; k < kTrials; k++) {
-        const T h = T(0.125 / (double)(1 << k));
-        T c = add(V, mul(h, dv));
-        if (un != 0) c = T(un);
-        c = clampv(c, T(-1), T(1));
-        nxt[(int64_t)k * P.var_cap + v] = c;
-        const bool fail = fabs((double)c - (double)V) >= 1.0;
-        if (!fail && kv == kTrials) kv = k;
+      unsat = warp_sum_i(unsat);
+      vfail = warp_sum_i(vfail);
+      if ((tid & 31) == 0) {
+        cnt[0][tid >> 5] = unsat;
+        cnt[1][tid >> 5] = vfail;
       }
-      kmax = max(kmax, kv);
-    }
-  }
-  kmax = warp_max_i(kmax);
-  if ((threadIdx.x & 31) == 0) sm.cnt[0][threadIdx.x >> 5] = kmax;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int km = 0;
+      const double et = block_sum<NT>(e, red);  // also completes the staging area
+      {
+        float4* __restrict__ dst = reinterpret_cast<float4*>(P.ux + ubase);
+        const float4* src = reinterpret_cast<const float4*>(stage);
+        for (int i = tid; i < ulen / 4; i += NT) dst[i] = src[i];
+      }
+      if (tid == 0) {
+        int tu = 0, tv = 0;
 #pragma unroll
-    for (int i = 0; i < NT / 32; i++) km = max(km, sm.cnt[0][i]);
-    if (km) atomicMax(sm.acc ? &sm.acc->kmax : &P.ctrl[sm.tile.inst].acc_kmax, km);
+        for (int i = 0; i < NT / 32; i++) {
+          tu += cnt[0][i];
+          tv += cnt[1][i];
+        }
+        if (tu) atomicAdd(&acc->loc, tu);
+        if (tv) atomicAdd(&acc->vfail, tv);
+        atomicAdd(&acc->energy, (unsigned long long)et);
+      }
+    }
+    trace_stamp(P, s, 3);
+
+    // ---- barrier 1 (split): phase B's own operands load during the wait
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(bar, 1u);
+    }
+    target += gridDim.x;
+    uint32_t w[kXpPairs];
+    T cv = T(0);
+    const int nv = has_v ? vtile.count : 0, v0 = has_v ? vtile.begin : 0;
+    const uint32_t* __restrict__ xd2 =
+        reinterpret_cast<const uint32_t*>(P.xdst + bbeg);  // positions, two per word
+    const int nb2 = blen / 2;
+    if (has_v) {
+#pragma unroll
+      for (int k = 0; k < kXpPairs; k++) {
+        const int q = tid + k * NT;
+        w[k] = q < nb2 ? __ldg(xd2 + q) : 0xFFFFFFFFu;
+      }
+      if (tid < nv) cv = V[v0 + tid];  // V(step) of the tile's variables
+    }
+    if (tid == 0) {
+      int ok = 1;
+      long long it = 0;
+      while (ld_acquire(bar) < target) {
+        if (++it > kBarrierSpinLimit) {
+          ok = 0;
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(kPollSleepNs);
+      }
+      __threadfence();
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    trace_stamp(P, s, 4);
+
+    // the step's counts of phase A, used by the decision after barrier 2
+    if (tid == 0) {
+      const volatile StepAcc* A = acc;
+      s_loc = A->loc;
+      s_vfail = A->vfail;
+      if (b == 0) {
+        s_energy = A->energy;
+        // every block has passed barrier 2 of step s-1, the last reader of the other slot
+        StepAcc* z = P.acc2 + ((s + 1) & 1);
+        z->loc = 0;
+        z->vfail = 0;
+        z->kmax = 0;
+        z->energy = 0ull;
+        z->arrive = 0ull;
+      }
+    }
+    trace_stamp(P, s, 5);
+
+    // ---- phase B
+    if (has_v) {
+      auto issue = [&](int q, uint32_t word) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const unsigned pos = h ? (word >> 16) : (word & 0xffffu);
+          const int p = 2 * q + h;
+          if (pos != kXpPad) cp_async4(bucket + pos, P.ux + s_src8[p >> 3] + (p & 7));
+        }
+      };
+#pragma unroll
+      for (int k = 0; k < kXpPairs; k++) {
+        const int q = tid + k * NT;
+        if (q < nb2) issue(q, w[k]);
+      }
+      for (int q = tid + kXpPairs * NT; q < nb2; q += NT) issue(q, __ldg(xd2 + q));
+      if (tid < nv) s_cur[tid] = cv;
+      for (int i = tid + NT; i < nv; i += NT) s_cur[i] = V[v0 + i];
+      cp_async_wait_all();
+      __syncthreads();
+      trace_stamp(P, s, 6);
+      T* __restrict__ nxt = P.cand + (int64_t)((set ^ 1) * kTrials) * P.var_cap + I.var0;
+      constexpr int VPP = NT / G;
+      const int grp = tid / G, lane = tid % G;
+      int kmax_b = 0;
+      for (int vb = 0; vb < nv; vb += VPP) {
+        const int i = vb + grp;
+        const bool valid = i < nv;
+        int s0 = 0, s1 = 0;
+        if (valid) {
+          s0 = s_vend[i];
+          s1 = s_vend[i + 1];
+        }
+        const T dv = tree_sum<T, G, true, int32_t>(bucket + s0, nullptr, s1 - s0, lane);
+        if (valid && lane == 0) {
+          const T Vv = s_cur[i];
+          const int8_t un = s_unit[i];
+          const int v = v0 + i;
+          int kv = kTrials;
+#pragma unroll
+          for (int k = 0; k < kTrials; k++) {
+            const T h = T(0.125 / (double)(1 << k));
+            T c = add(Vv, mul(h, dv));
+            if (un != 0) c = T(un);
+            c = clampv(c, T(-1), T(1));
+            nxt[(int64_t)k * P.var_cap + v] = c;
+            const bool fail = fabs((double)c - (double)Vv) >= 1.0;
+            if (!fail && kv == kTrials) kv = k;
+          }
+          kmax_b = max(kmax_b, kv);
+        }
+      }
+      kmax_b = warp_max_i(kmax_b);
+      if ((tid & 31) == 0) cnt[0][tid >> 5] = kmax_b;
+    }
+    trace_stamp(P, s, 7);
+
+    // ---- barrier 2 (carries the largest trial index) and the step decision
+    __syncthreads();
+    if (tid == 0) {
+      int km = 0;
+      if (has_v) {
+#pragma unroll
+        for (int i = 0; i < NT / 32; i++) km = max(km, cnt[0][i]);
+      }
+      __threadfence();
+      atomicAdd(&acc->arrive, 1ull << (kArriveBits * km));
+      int ok = 1, kmax = 0;
+      long long it = 0;
+      for (;;) {
+        const unsigned long long a = ld_acquire64(&acc->arrive);
+        unsigned int n = 0;
+        kmax = 0;
+#pragma unroll
+        for (int k = 0; k <= kTrials; k++) {
+          const unsigned int f =
+              (unsigned int)(a >> (kArriveBits * k)) & ((1u << kArriveBits) - 1);
+          n += f;
+          if (f) kmax = k;
+        }
+        if (n >= gridDim.x) break;
+        if (++it > kBarrierSpinLimit) {
+          ok = 0;
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(kPollSleepNs);
+      }
+      __threadfence();
+      s_ok = ok;
+      trace_stamp(P, s, 8);
+      const int loc = s_loc, vfail = s_vfail;
+      const StepDecision d = decide(loc, vfail, kmax, lc.step, I.max_steps);
+      if (b == 0) {
+        InstCtrl* S = P.ctrl + ii;
+        if (loc < lc.best_loc) {
+          S->best_loc = loc;
+          S->best_t = lc.t;
+          lc.best_loc = loc;
+          lc.best_t = lc.t;
+        }
+        if (d.status == 1) {
+          S->solved_step = lc.step;
+          S->solved_t = lc.t;
+          S->sol_set = set;
+          S->sol_k = kcur;
+        }
+        S->loc = loc;
+        S->vfail = vfail;
+        S->energy = (double)s_energy * (1.0 / kEnergyUnitF32);
+        S->t = __dadd_rn(lc.t, d.ht);
+        S->step = lc.step + 1;
+        S->set = set ^ 1;
+        S->kcur = d.kacc;
+        S->h_state = d.hs;
+        S->pending = 1;
+        if (d.status) {
+          S->done = d.status;
+          atomicSub(P.active, 1);
+          const int pos = atomicAdd(P.ring_tail, 1);
+          P.ring[pos % P.ring_cap] = ii;
+        }
+        __threadfence();
+      }
+      lc.t = __dadd_rn(lc.t, d.ht);
+      lc.done = d.status;
+      lc.step += 1;
+      lc.set = set ^ 1;
+      lc.kcur = d.kacc;
+      lc.h = d.hs;
+      lc.pending = 1;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    trace_stamp(P, s, 9);
   }
-  __syncthreads();
 }
 
 }  // namespace dmm

@@ -122,8 +122,8 @@ inline int blocks_for(int64_t work, int per = kThreads, int cap = 148 * 16) {
 constexpr int kMinClauseTile = 256;  // smallest clause tile (bounds the tile tables)
 constexpr int kMinVarTile = 32;      // smallest variable tile
 constexpr int kPersistThreads = 1024;  // block size of the cooperative step kernel
-constexpr int kXpSmemMax = 200 * 1024;  // dynamic shared memory of the staged form, at most
-constexpr int kMiscInts = 32;            // misc_d_: 128 bytes
+constexpr int kXpSmemMax = 220 * 1024;  // dynamic shared memory of the staged form, at most
+constexpr int kMiscInts = 48;            // misc_d_: 192 bytes
 constexpr int kMiscLaunch = 16;          // misc_d_ index of the per-launch area (byte 64)
 constexpr int kMiscAcc2 = 20;            // misc_d_ index of the StepAcc pair (byte 80)
 }  // namespace
@@ -213,7 +213,7 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   DMM_CUDA(cudaMalloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&live_d_, I * sizeof(int32_t)));
   DMM_CUDA(cudaMalloc(&order_d_, I * sizeof(int32_t)));
-  // [0] live formulas, [1] error flag, [3] k_inst queue; bytes 64..127: grid-barrier
+  // [0] live formulas, [1] error flag, [3] k_inst queue; bytes 64..191: grid-barrier
   // counter and the two step accumulators of the single-formula form (zeroed per launch)
   DMM_CUDA(cudaMalloc(&misc_d_, kMiscInts * sizeof(int32_t)));
   DMM_CUDA(cudaMemsetAsync(misc_d_, 0, kMiscInts * sizeof(int32_t), stream_));
@@ -742,24 +742,36 @@ static int occupancy_blocks(const void* fn, int threads, size_t smem = 0) {
   return std::max(1, b);
 }
 
-// XP: staged form; ONE: single-formula form (both FP32 only)
-template <bool XP, bool ONE>
+// ONE: single-formula form (FP32 only)
+template <bool ONE>
 static const void* persist_fn_x(dmm_precision prec, int G) {
   if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads>;
   switch (G) {
-    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, XP, ONE>;
-    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, XP, ONE>;
-    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads, XP, ONE>;
-    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads, XP, ONE>;
-    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads, XP, ONE>;
-    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads, XP, ONE>;
+    case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, ONE>;
+    case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, ONE>;
+    case 4: return (const void*)k_persist<float, 4, false, true, kPersistThreads, ONE>;
+    case 8: return (const void*)k_persist<float, 8, false, true, kPersistThreads, ONE>;
+    case 16: return (const void*)k_persist<float, 16, false, true, kPersistThreads, ONE>;
+    default: return (const void*)k_persist<float, 32, false, true, kPersistThreads, ONE>;
+  }
+}
+
+// the staged form (FP32, single formula)
+static const void* staged_fn(int G) {
+  switch (G) {
+    case 1: return (const void*)k_staged<1, kPersistThreads>;
+    case 2: return (const void*)k_staged<2, kPersistThreads>;
+    case 4: return (const void*)k_staged<4, kPersistThreads>;
+    case 8: return (const void*)k_staged<8, kPersistThreads>;
+    case 16: return (const void*)k_staged<16, kPersistThreads>;
+    default: return (const void*)k_staged<32, kPersistThreads>;
   }
 }
 
 const void* Pack::persist_fn() const {
-  if (xp_active_) return persist_fn_x<true, true>(prec_, tun_.var_group);
-  if (one_active_) return persist_fn_x<false, true>(prec_, tun_.var_group);
-  return persist_fn_x<false, false>(prec_, tun_.var_group);
+  if (xp_active_) return staged_fn(tun_.var_group);
+  if (one_active_) return persist_fn_x<true>(prec_, tun_.var_group);
+  return persist_fn_x<false>(prec_, tun_.var_group);
 }
 
 // Tables of the staged form (dmm_xpose.cuh) for formula idx with clause tiles of TC and
@@ -820,7 +832,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
     boff[b + 1] = boff[b] + (int32_t)acc;
   }
   // distinct variables of every clause tile (ascending) and the tile-local literals
-  std::vector<int32_t> dlist, doff(nct + 1, 0), where(n, -1);
+  std::vector<int32_t> dlist, doff(2 * nct, 0), where(n, -1);
   std::vector<int16_t> llit(L);
   int64_t sv_max = 0;
   dlist.reserve(L);
@@ -837,8 +849,9 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
     std::sort(dlist.begin() + d0, dlist.end());
     const int64_t nd = (int64_t)(dlist.size() - d0);
     if (nd > 32767) return DMM_OK;  // 16-bit signed local literals
-    sv_max = std::max(sv_max, nd);
-    doff[t + 1] = (int32_t)dlist.size();
+    sv_max = std::max(sv_max, (nd + 3) & ~int64_t(3));
+    doff[2 * t] = (int32_t)d0;
+    doff[2 * t + 1] = (int32_t)nd;
     for (size_t i = d0; i < dlist.size(); i++) where[dlist[i]] = -2 - (int32_t)(i - d0);
     for (int s = s_lo; s < s_hi; s++) {
       const int v = std::abs(lits[s]) - 1;
@@ -846,6 +859,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
       llit[s] = (int16_t)(lits[s] > 0 ? loc + 1 : -(loc + 1));
     }
     for (size_t i = d0; i < dlist.size(); i++) where[dlist[i]] = t;
+    while (dlist.size() % 4) dlist.push_back(0);  // 16-byte aligned tile lists
   }
   // staging position of every slot (ascending slot within a chunk) and its bucket entry
   std::vector<uint16_t> spos(L), dst(boff[nvt], kXpPad);
@@ -871,7 +885,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   const int bk_cap = (int)std::max<int64_t>(std::max(st_max, bk_max), 8);
   const int smem = xp_layout(sv_cap, bk_cap, TV).total;
   if (smem > kXpSmemMax) return DMM_OK;
-  if (occupancy_blocks(persist_fn_x<true, true>(prec_, tun_.var_group), kPersistThreads, smem) * sms_ != grid_p_)
+  if (occupancy_blocks(staged_fn(tun_.var_group), kPersistThreads, smem) * sms_ != grid_p_)
     return DMM_OK;
   struct Up {
     int which;
