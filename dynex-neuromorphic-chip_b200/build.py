@@ -25,8 +25,9 @@ OBJ_DIR = os.path.join(HERE, "lib", "obj")
 LIB = os.path.join(LIB_DIR, "libdmm.so")
 CLI = os.path.join(BIN_DIR, "dynex")
 
-SOURCES = ["pack.cu", "cnf.cpp", "capi.cpp", "server.cpp", "noalloc.cu"]
-HEADERS = ["dmm_device.cuh", "dmm_kernels.cuh", "dmm_step.cuh", "dmm_inst.cuh", "dmm_pack.h"]
+SOURCES = ["pack.cu", "cnf.cpp", "capi.cpp", "server.cpp", "noalloc.cu", "devmem.cpp"]
+HEADERS = ["dmm_device.cuh", "dmm_kernels.cuh", "dmm_step.cuh", "dmm_inst.cuh", "dmm_xpose.cuh", "dmm_xprep.cuh",
+           "dmm_pack.h", "devmem.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

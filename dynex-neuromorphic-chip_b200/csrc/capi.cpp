@@ -5,6 +5,7 @@
 #include <new>
 #include <vector>
 
+#include "devmem.h"
 #include "dmm_pack.h"
 
 using dmm::InstCtrl;
@@ -79,6 +80,8 @@ void dmm_params_default(dmm_params* p) {
   p->xl_max = 10000;  // dynex.cc:140
   p->reserved = 0;
 }
+
+void dmm_release_cached_memory(void) { dmm::release_cached(); }
 
 int32_t dmm_device_count(void) {
   int n = 0;

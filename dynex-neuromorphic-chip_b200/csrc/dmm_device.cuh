@@ -121,7 +121,8 @@ struct PackView {
   // phase trace of the cooperative kernel (null when off): trace[(s * kTraceK + k) * grid +
   // block] = %globaltimer at step s's point k: 0 start, 1 clause tile loaded, 2 voltages
   // gathered, 3 phase A done, 4 past barrier 1, 5 variable tile loaded, 6 bucket filled,
-  // 7 phase B done, 8 past barrier 2, 9 phase F done
+  // 7 phase B done, 8 past barrier 2, 9 phase F done; followed by the same layout of SM
+  // clock counts
   long long* trace;
   int32_t trace_steps;
 };

@@ -107,7 +107,8 @@ class Pack {
   dmm_status time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double* ms);
   // One cooperative launch of nsteps steps with %globaltimer stamps at kTraceK points of
   // every step; out[2k], out[2k+1] = mean and max over blocks of the microseconds from
-  // point k to point k+1 (point kTraceK: the next step's start), averaged over steps.
+  // point k to point k+1 (point kTraceK: the next step's start), averaged over steps;
+  // out[2 kTraceK] = SM clock (MHz).
   dmm_status trace_phases(int32_t nsteps, double* out);
   // Raises DMM_ERR_CUDA when a cooperative launch reported a grid-barrier timeout.
   dmm_status check_error();
@@ -178,7 +179,8 @@ class Pack {
   // staged form (single FP32 formula of 3-literal clauses on the cooperative path)
   bool xp_active_ = false;
   bool one_active_ = false;  // single FP32 formula on the cooperative path
-  enum { kXpDlist, kXpDoff, kXpLlit, kXpSpos, kXpUx, kXpUbase, kXpBoff, kXpSrc8, kXpDst, kXpBufs };
+  enum { kXpDlist, kXpDoff, kXpLlit, kXpSpos, kXpUx, kXpUbase, kXpBoff, kXpSrc8, kXpDst,
+         kXpScratch, kXpBufs };
   void* xbuf_[kXpBufs] = {};
   int64_t xbuf_cap_[kXpBufs] = {};
   int32_t xsv_cap_ = 0, xbk_cap_ = 0, xtv_cap_ = 0, xsmem_ = 0;

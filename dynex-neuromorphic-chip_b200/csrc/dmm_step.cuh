@@ -56,7 +56,9 @@ __device__ __forceinline__ void trace_stamp(const PackView<T>& P, int s, int k) 
   if (P.trace && threadIdx.x == 0 && s < P.trace_steps) {
     long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    P.trace[((int64_t)s * kTraceK + k) * gridDim.x + blockIdx.x] = t;
+    const int64_t at = ((int64_t)s * kTraceK + k) * gridDim.x + blockIdx.x;
+    P.trace[at] = t;
+    P.trace[at + (int64_t)P.trace_steps * kTraceK * gridDim.x] = clock64();
   }
 }
 

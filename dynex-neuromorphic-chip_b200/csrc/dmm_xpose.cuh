@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(NT, 1)
         stage[p2] = u2;
         unsat += !(C < T(0.5));
         vfail += !ss;
-        e += (double)C * kEnergyUnitF32;
+        e += (double)C;  // exact: multiples of 2^-25, scaled once per block
         return C;
       };
       auto group = [&](const Group4& q, int g) {
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(NT, 1)
         cnt[0][tid >> 5] = unsat;
         cnt[1][tid >> 5] = vfail;
       }
-      const double et = block_sum<NT>(e, red);  // also completes the staging area
+      const double et = block_sum<NT>(e, red) * kEnergyUnitF32;  // also completes the staging area
       {
         float4* __restrict__ dst = reinterpret_cast<float4*>(P.ux + ubase);
         const float4* src = reinterpret_cast<const float4*>(stage);

@@ -8,7 +8,9 @@
 
 #include "dmm_inst.cuh"
 #include "dmm_step.cuh"
+#include "dmm_xprep.cuh"
 #include "dmm_pack.h"
+#include "devmem.h"
 
 namespace dmm {
 
@@ -152,12 +154,12 @@ Pack::~Pack() {
                   stage_,   aux_ctiles_d_, aux_vtiles_d_, flush_, live_d_, misc_d_, order_d_,
                   upos_,    trace_};
   for (void* p : ptrs)
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
   for (void* p : xbuf_)
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
-  if (pinned_) cudaFreeHost(pinned_);
+  if (pinned_) pinned_free(pinned_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -187,35 +189,35 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   const int64_t V = caps_.vars, C = caps_.clauses, S = caps_.slots, I = caps_.insts;
   ctile_cap_ = C / kMinClauseTile + I + 1;
   vtile_cap_ = V / kMinVarTile + I + 1;
-  DMM_CUDA(cudaMalloc(&Xs_, C * tsize_));
-  DMM_CUDA(cudaMalloc(&Xl_, C * tsize_));
-  DMM_CUDA(cudaMalloc(&Cp_, C * tsize_));
-  if (with_alpha_cm) DMM_CUDA(cudaMalloc(&alpha_cm_, C * tsize_));
-  DMM_CUDA(cudaMalloc(&coff_, C * 4));
-  DMM_CUDA(cudaMalloc(&lit_, S * 4));
-  DMM_CUDA(cudaMalloc(&vslot_, S * 4));
-  DMM_CUDA(cudaMalloc(&upos_, S * 4));
-  DMM_CUDA(cudaMalloc(&u_, S * tsize_));
-  DMM_CUDA(cudaMalloc(&cand_, 2 * kTrials * V * tsize_));
-  DMM_CUDA(cudaMalloc(&vend_, V * 4));
-  DMM_CUDA(cudaMalloc(&fill_, V * 4));
-  DMM_CUDA(cudaMalloc(&unit_, V));
-  DMM_CUDA(cudaMalloc(&epart_, ctile_cap_ * sizeof(double)));
-  DMM_CUDA(cudaMalloc(&inst_d_, I * sizeof(InstDesc)));
-  DMM_CUDA(cudaMalloc(&ctrl_d_, I * sizeof(InstCtrl)));
-  DMM_CUDA(cudaMalloc(&ctiles_d_, ctile_cap_ * sizeof(Tile)));
-  DMM_CUDA(cudaMalloc(&vtiles_d_, vtile_cap_ * sizeof(Tile)));
-  DMM_CUDA(cudaMalloc(&ntiles_d_, 4 * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&queue_d_, 2 * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&active_d_, sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&ring_d_, I * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&ring_tail_d_, 4 * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&live_d_, I * sizeof(int32_t)));
-  DMM_CUDA(cudaMalloc(&order_d_, I * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&Xs_, C * tsize_));
+  DMM_CUDA(dev_alloc(&Xl_, C * tsize_));
+  DMM_CUDA(dev_alloc(&Cp_, C * tsize_));
+  if (with_alpha_cm) DMM_CUDA(dev_alloc(&alpha_cm_, C * tsize_));
+  DMM_CUDA(dev_alloc(&coff_, C * 4));
+  DMM_CUDA(dev_alloc(&lit_, S * 4));
+  DMM_CUDA(dev_alloc(&vslot_, S * 4));
+  DMM_CUDA(dev_alloc(&upos_, S * 4));
+  DMM_CUDA(dev_alloc(&u_, S * tsize_));
+  DMM_CUDA(dev_alloc(&cand_, 2 * kTrials * V * tsize_));
+  DMM_CUDA(dev_alloc(&vend_, V * 4));
+  DMM_CUDA(dev_alloc(&fill_, V * 4));
+  DMM_CUDA(dev_alloc(&unit_, V));
+  DMM_CUDA(dev_alloc(&epart_, ctile_cap_ * sizeof(double)));
+  DMM_CUDA(dev_alloc(&inst_d_, I * sizeof(InstDesc)));
+  DMM_CUDA(dev_alloc(&ctrl_d_, I * sizeof(InstCtrl)));
+  DMM_CUDA(dev_alloc(&ctiles_d_, ctile_cap_ * sizeof(Tile)));
+  DMM_CUDA(dev_alloc(&vtiles_d_, vtile_cap_ * sizeof(Tile)));
+  DMM_CUDA(dev_alloc(&ntiles_d_, 4 * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&queue_d_, 2 * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&active_d_, sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&ring_d_, I * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&ring_tail_d_, 4 * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&live_d_, I * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&order_d_, I * sizeof(int32_t)));
   // [0] live formulas, [1] error flag, [3] k_inst queue; bytes 64..191: grid-barrier
   // counter and the two step accumulators of the single-formula form (zeroed per launch)
-  DMM_CUDA(cudaMalloc(&misc_d_, kMiscInts * sizeof(int32_t)));
+  DMM_CUDA(dev_alloc(&misc_d_, kMiscInts * sizeof(int32_t)));
   DMM_CUDA(cudaMemsetAsync(misc_d_, 0, kMiscInts * sizeof(int32_t), stream_));
   DMM_CUDA(cudaMemsetAsync(ctrl_d_, 0, I * sizeof(InstCtrl), stream_));
   DMM_CUDA(cudaMemsetAsync(ntiles_d_, 0, 4 * sizeof(int32_t), stream_));
@@ -293,10 +295,10 @@ int32_t Pack::free_insts() const {
 
 dmm_status Pack::ensure_stage(int64_t doubles) {
   if (doubles <= stage_cap_) return DMM_OK;
-  if (stage_) DMM_CUDA(cudaFree(stage_));
+  if (stage_) dev_free(stage_);
   stage_ = nullptr;
   stage_cap_ = 0;
-  DMM_CUDA(cudaMalloc(&stage_, doubles * sizeof(double)));
+  DMM_CUDA(dev_alloc(&stage_, doubles * sizeof(double)));
   stage_cap_ = doubles;
   return DMM_OK;
 }
@@ -368,9 +370,9 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
   }
   const int64_t need = n / (kThreads * 8) + 64;
   if (need > scan_tmp_cap_) {
-    if (scan_tmp_) DMM_CUDA(cudaFree(scan_tmp_));
+    if (scan_tmp_) dev_free(scan_tmp_);
     scan_tmp_ = nullptr;
-    DMM_CUDA(cudaMalloc(&scan_tmp_, need * 2 * sizeof(int32_t)));
+    DMM_CUDA(dev_alloc(&scan_tmp_, need * 2 * sizeof(int32_t)));
     scan_tmp_cap_ = need;
   }
   DMM_TRY(scan_inclusive(vend, n, scan_tmp_, stream_));
@@ -775,145 +777,90 @@ const void* Pack::persist_fn() const {
 }
 
 // Tables of the staged form (dmm_xpose.cuh) for formula idx with clause tiles of TC and
-// variable tiles of TV.  Leaves *ok false (and the plain tile code in use) when the
-// formula or its tiles do not fit the form's 16-bit indices or shared memory.
+// variable tiles of TV, built on the device (dmm_xprep.cuh).  Leaves *ok false (and the
+// plain tile code in use) when the formula or its tiles do not fit the form's 16-bit
+// indices or shared memory.
 dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   *ok = false;
   const InstDesc& I = inst_h_[idx];
   if (prec_ != DMM_FP32 || !I.k3) return DMM_OK;
   const int m = I.m, n = I.n, L = I.nslots;
   const int nct = (m + TC - 1) / TC, nvt = (n + TV - 1) / TV;
-  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_) return DMM_OK;
-  std::vector<int32_t> lits(L), vsl(L);
-  DMM_CUDA(cudaMemcpyAsync(lits.data(), lit_ + I.slot0, (size_t)L * 4, cudaMemcpyDeviceToHost, stream_));
-  DMM_CUDA(cudaMemcpyAsync(vsl.data(), vslot_ + I.slot0, (size_t)L * 4, cudaMemcpyDeviceToHost, stream_));
+  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_ || nvt > kXprepThreads)
+    return DMM_OK;
+  const int W = (n + 31) / 32;
+  const int smem_k = (nvt + 2 * W) * 4;
+  if (smem_k > kXpSmemMax) return DMM_OK;
+  const int64_t pairs = (int64_t)nct * nvt;
+  const int64_t ux_cap = (int64_t)L + 8 * pairs;  // sector padding: < 8 per chunk
+  if (ux_cap > INT32_MAX) return DMM_OK;
+  // scratch: cnt, sb, bt (pairs each), st, dcnt (nct each), out (8)
+  const int64_t scratch_ints = 3 * pairs + 2 * (int64_t)nct + 8;
+  const int64_t bytes[kXpBufs] = {
+      ((int64_t)L + 4 * nct) * 4,  // dlist
+      2 * (int64_t)nct * 4,        // doff
+      (int64_t)L * 2,              // llit
+      (int64_t)L * 2,              // spos
+      ux_cap * 4,                  // ux
+      ((int64_t)nct + 1) * 4,      // ubase
+      ((int64_t)nvt + 1) * 4,      // boff
+      (ux_cap / 8 + 1) * 4,        // src8
+      ux_cap * 2,                  // dst
+      scratch_ints * 4};           // scratch
+  for (int i = 0; i < kXpBufs; i++) {
+    const int64_t want = std::max<int64_t>(bytes[i], 16);
+    if (want > xbuf_cap_[i]) {
+      if (xbuf_[i]) dev_free(xbuf_[i]);
+      xbuf_[i] = nullptr;
+      xbuf_cap_[i] = 0;
+      DMM_CUDA(dev_alloc(&xbuf_[i], want));
+      xbuf_cap_[i] = want;
+    }
+  }
+  int* scr = static_cast<int*>(xbuf_[kXpScratch]);
+  int* cnt = scr;
+  int* sb = cnt + pairs;
+  int* bt = sb + pairs;
+  int* st = bt + pairs;
+  int* dcnt = st + nct;
+  int* out = dcnt + nct;
+  auto* dlist = static_cast<int32_t*>(xbuf_[kXpDlist]);
+  auto* doff = static_cast<int32_t*>(xbuf_[kXpDoff]);
+  auto* llit = static_cast<int16_t*>(xbuf_[kXpLlit]);
+  auto* spos = static_cast<uint16_t*>(xbuf_[kXpSpos]);
+  auto* ubase = static_cast<int32_t*>(xbuf_[kXpUbase]);
+  auto* boff = static_cast<int32_t*>(xbuf_[kXpBoff]);
+  auto* src8 = static_cast<int32_t*>(xbuf_[kXpSrc8]);
+  auto* dst = static_cast<uint16_t*>(xbuf_[kXpDst]);
+  const int32_t* lit = lit_ + I.slot0;
+  const int32_t* upos = upos_ + I.slot0;
+  const int32_t* vend = vend_ + I.var0;
+  DMM_CUDA(cudaMemsetAsync(dlist, 0, bytes[kXpDlist], stream_));
+  DMM_CUDA(cudaMemsetAsync(dst, 0xFF, bytes[kXpDst], stream_));
+  if (smem_k > 48 * 1024) {
+    DMM_CUDA(cudaFuncSetAttribute(k_xp_count<kXprepThreads>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem_k));
+    DMM_CUDA(cudaFuncSetAttribute(k_xp_fill<kXprepThreads>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem_k));
+  }
+  k_xp_count<kXprepThreads><<<nct, kXprepThreads, smem_k, stream_>>>(lit, L, TC, TV, nvt, W, cnt,
+                                                                     sb, st, dcnt, spos);
+  k_xp_scan<kXprepThreads><<<1, kXprepThreads, 0, stream_>>>(nct, nvt, cnt, st, dcnt, ubase,
+                                                             doff, bt, boff, out);
+  k_xp_fill<kXprepThreads><<<nct, kXprepThreads, smem_k, stream_>>>(
+      lit, upos, vend, L, TC, TV, nct, nvt, W, sb, ubase, doff, bt, boff, dlist, llit, spos, dst,
+      src8);
+  DMM_CUDA(cudaGetLastError());
+  int h[8];
+  DMM_CUDA(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, stream_));
   DMM_CUDA(cudaStreamSynchronize(stream_));
-  auto pad8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
-  auto tile_of = [&](int s) { return (s / 3) / TC; };
-  auto vtile_of = [&](int s) { return (std::abs(lits[s]) - 1) / TV; };
-  // variable-major position of every slot; start of each variable tile's lists
-  std::vector<int32_t> vpos(L), jb(nvt + 1, 0);
-  for (int j = 0; j < L; j++) vpos[vsl[j]] = j;
-  {
-    std::vector<int32_t> per_tile(nvt, 0);
-    for (int s = 0; s < L; s++) per_tile[vtile_of(s)]++;
-    for (int b = 0; b < nvt; b++) {
-      if (per_tile[b] >= (int32_t)kXpPad) return DMM_OK;  // 16-bit bucket positions
-      jb[b + 1] = jb[b] + per_tile[b];
-    }
-  }
-  std::vector<int32_t> cnt((size_t)nct * nvt, 0);
-  for (int s = 0; s < L; s++) cnt[(size_t)tile_of(s) * nvt + vtile_of(s)]++;
-  // staging area of clause tile t: chunk b at sb[t][b], sector-padded
-  std::vector<int32_t> sb((size_t)nct * nvt), ubase(nct + 1, 0);
-  int64_t st_max = 0;
-  for (int t = 0; t < nct; t++) {
-    int64_t acc = 0;
-    for (int b = 0; b < nvt; b++) {
-      sb[(size_t)t * nvt + b] = (int32_t)acc;
-      acc += pad8(cnt[(size_t)t * nvt + b]);
-    }
-    if (acc > 65535) return DMM_OK;  // 16-bit staging positions
-    st_max = std::max(st_max, acc);
-    if ((int64_t)ubase[t] + acc > INT32_MAX) return DMM_OK;
-    ubase[t + 1] = ubase[t] + (int32_t)acc;
-  }
-  // bucket of variable tile b: chunk of clause tile t at bt[b][t] (from boff[b])
-  std::vector<int32_t> bt((size_t)nvt * nct), boff(nvt + 1, 0);
-  int64_t bk_max = 0;
-  for (int b = 0; b < nvt; b++) {
-    int64_t acc = 0;
-    for (int t = 0; t < nct; t++) {
-      bt[(size_t)b * nct + t] = (int32_t)acc;
-      acc += pad8(cnt[(size_t)t * nvt + b]);
-    }
-    bk_max = std::max(bk_max, acc);
-    if ((int64_t)boff[b] + acc > INT32_MAX) return DMM_OK;
-    boff[b + 1] = boff[b] + (int32_t)acc;
-  }
-  // distinct variables of every clause tile (ascending) and the tile-local literals
-  std::vector<int32_t> dlist, doff(2 * nct, 0), where(n, -1);
-  std::vector<int16_t> llit(L);
-  int64_t sv_max = 0;
-  dlist.reserve(L);
-  for (int t = 0; t < nct; t++) {
-    const int s_lo = 3 * t * TC, s_hi = std::min(L, 3 * (t + 1) * TC);
-    const size_t d0 = dlist.size();
-    for (int s = s_lo; s < s_hi; s++) {
-      const int v = std::abs(lits[s]) - 1;
-      if (where[v] != t) {
-        where[v] = t;
-        dlist.push_back(v);
-      }
-    }
-    std::sort(dlist.begin() + d0, dlist.end());
-    const int64_t nd = (int64_t)(dlist.size() - d0);
-    if (nd > 32767) return DMM_OK;  // 16-bit signed local literals
-    sv_max = std::max(sv_max, (nd + 3) & ~int64_t(3));
-    doff[2 * t] = (int32_t)d0;
-    doff[2 * t + 1] = (int32_t)nd;
-    for (size_t i = d0; i < dlist.size(); i++) where[dlist[i]] = -2 - (int32_t)(i - d0);
-    for (int s = s_lo; s < s_hi; s++) {
-      const int v = std::abs(lits[s]) - 1;
-      const int loc = -2 - where[v];
-      llit[s] = (int16_t)(lits[s] > 0 ? loc + 1 : -(loc + 1));
-    }
-    for (size_t i = d0; i < dlist.size(); i++) where[dlist[i]] = t;
-    while (dlist.size() % 4) dlist.push_back(0);  // 16-byte aligned tile lists
-  }
-  // staging position of every slot (ascending slot within a chunk) and its bucket entry
-  std::vector<uint16_t> spos(L), dst(boff[nvt], kXpPad);
-  std::vector<int32_t> src8(boff[nvt] / 8);
-  {
-    std::vector<int32_t> cur(sb);
-    for (int s = 0; s < L; s++) {
-      const int t = tile_of(s), b = vtile_of(s);
-      const int32_t q = cur[(size_t)t * nvt + b]++;
-      spos[s] = (uint16_t)q;
-      const int64_t p = (int64_t)boff[b] + bt[(size_t)b * nct + t] + (q - sb[(size_t)t * nvt + b]);
-      dst[p] = (uint16_t)(vpos[s] - jb[b]);
-    }
-    for (int b = 0; b < nvt; b++)
-      for (int t = 0; t < nct; t++) {
-        const int64_t g0 = ((int64_t)boff[b] + bt[(size_t)b * nct + t]) / 8;
-        const int64_t ng = pad8(cnt[(size_t)t * nvt + b]) / 8;
-        for (int64_t k = 0; k < ng; k++)
-          src8[g0 + k] = ubase[t] + sb[(size_t)t * nvt + b] + (int32_t)(8 * k);
-      }
-  }
-  const int sv_cap = (int)std::max<int64_t>(sv_max, 1);
-  const int bk_cap = (int)std::max<int64_t>(std::max(st_max, bk_max), 8);
+  if (h[0] != 0) return DMM_OK;
+  const int sv_cap = std::max(h[1], 4);
+  const int bk_cap = std::max(h[2], 8);
   const int smem = xp_layout(sv_cap, bk_cap, TV).total;
   if (smem > kXpSmemMax) return DMM_OK;
   if (occupancy_blocks(staged_fn(tun_.var_group), kPersistThreads, smem) * sms_ != grid_p_)
     return DMM_OK;
-  struct Up {
-    int which;
-    const void* src;
-    int64_t bytes;
-  };
-  const Up ups[] = {{kXpDlist, dlist.data(), (int64_t)dlist.size() * 4},
-                    {kXpDoff, doff.data(), (int64_t)doff.size() * 4},
-                    {kXpLlit, llit.data(), (int64_t)llit.size() * 2},
-                    {kXpSpos, spos.data(), (int64_t)spos.size() * 2},
-                    {kXpUx, nullptr, (int64_t)ubase[nct] * 4},
-                    {kXpUbase, ubase.data(), (int64_t)ubase.size() * 4},
-                    {kXpBoff, boff.data(), (int64_t)boff.size() * 4},
-                    {kXpSrc8, src8.data(), (int64_t)src8.size() * 4},
-                    {kXpDst, dst.data(), (int64_t)dst.size() * 2}};
-  for (const Up& u : ups) {
-    const int64_t bytes = std::max<int64_t>(u.bytes, 16);
-    if (bytes > xbuf_cap_[u.which]) {
-      if (xbuf_[u.which]) DMM_CUDA(cudaFree(xbuf_[u.which]));
-      xbuf_[u.which] = nullptr;
-      xbuf_cap_[u.which] = 0;
-      DMM_CUDA(cudaMalloc(&xbuf_[u.which], bytes));
-      xbuf_cap_[u.which] = bytes;
-    }
-    if (u.src && u.bytes > 0)
-      DMM_CUDA(cudaMemcpyAsync(xbuf_[u.which], u.src, u.bytes, cudaMemcpyHostToDevice, stream_));
-  }
-  DMM_CUDA(cudaStreamSynchronize(stream_));
   xsv_cap_ = sv_cap;
   xbk_cap_ = bk_cap;
   xtv_cap_ = TV;
@@ -1152,9 +1099,9 @@ dmm_status Pack::launch_steps(int32_t nsteps) {
 
 dmm_status Pack::ensure_flush(int64_t flush_bytes) {
   if (flush_bytes > flush_cap_) {
-    if (flush_) DMM_CUDA(cudaFree(flush_));
+    if (flush_) dev_free(flush_);
     flush_ = nullptr;
-    DMM_CUDA(cudaMalloc(&flush_, flush_bytes));
+    DMM_CUDA(dev_alloc(&flush_, flush_bytes));
     flush_cap_ = flush_bytes;
   }
   return DMM_OK;
@@ -1188,11 +1135,12 @@ dmm_status Pack::trace_phases(int32_t nsteps, double* out) {
     return DMM_ERR_STATE;
   }
   constexpr int K = kTraceK;
-  const int64_t need = (int64_t)nsteps * K * grid_p_;
+  const int64_t half = (int64_t)nsteps * K * grid_p_;
+  const int64_t need = 2 * half;  // timer stamps, then clock counts
   if (need > trace_cap_) {
-    if (trace_) DMM_CUDA(cudaFree(trace_));
+    if (trace_) dev_free(trace_);
     trace_ = nullptr;
-    DMM_CUDA(cudaMalloc(&trace_, need * sizeof(long long)));
+    DMM_CUDA(dev_alloc(&trace_, need * sizeof(long long)));
     trace_cap_ = need;
   }
   DMM_CUDA(cudaMemsetAsync(trace_, 0, need * sizeof(long long), stream_));
@@ -1238,15 +1186,22 @@ dmm_status Pack::trace_phases(int32_t nsteps, double* out) {
     out[2 * k] = used ? mean[k] / used / 1000.0 : 0.0;  // microseconds
     out[2 * k + 1] = used ? mx[k] / used / 1000.0 : 0.0;
   }
+  // SM clock of block 0 over the traced steps
+  out[2 * K] = 0.0;
+  if (used > 0) {
+    const long long t0 = at(0, 0, 0), t1 = at(used, 0, 0);
+    const long long c0 = h[half + 0], c1 = h[half + (int64_t)used * K * G];
+    if (t1 > t0) out[2 * K] = (double)(c1 - c0) / (double)(t1 - t0) * 1000.0;  // MHz
+  }
   return DMM_OK;
 }
 
 dmm_status Pack::profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t) {
   DMM_CUDA(cudaSetDevice(dev_));
   if (flush_bytes > flush_cap_) {
-    if (flush_) DMM_CUDA(cudaFree(flush_));
+    if (flush_) dev_free(flush_);
     flush_ = nullptr;
-    DMM_CUDA(cudaMalloc(&flush_, flush_bytes));
+    DMM_CUDA(dev_alloc(&flush_, flush_bytes));
     flush_cap_ = flush_bytes;
   }
   for (int32_t s = 0; s < nsteps; s++) {
@@ -1282,7 +1237,7 @@ dmm_status Pack::run(double wall_s, int64_t* steps_launched, bool* timed_out,
   DMM_CUDA(cudaSetDevice(dev_));
   *timed_out = false;
   if (steps_launched) *steps_launched = 0;
-  if (!pinned_) DMM_CUDA(cudaMallocHost(&pinned_, 4 * sizeof(int32_t)));
+  if (!pinned_) DMM_CUDA(pinned_alloc(&pinned_, 4 * sizeof(int32_t)));
   const auto t0 = std::chrono::steady_clock::now();
   auto elapsed = [&]() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1373,11 +1328,11 @@ dmm_status Pack::rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, d
   for (int32_t b = 0; b < I.n; b += TV) vt.push_back(Tile{idx, b, std::min(TV, I.n - b), 0});
   const int64_t need = std::max<int64_t>(std::max(ct.size(), vt.size()), 1);
   if (need > aux_cap_) {
-    if (aux_ctiles_d_) DMM_CUDA(cudaFree(aux_ctiles_d_));
-    if (aux_vtiles_d_) DMM_CUDA(cudaFree(aux_vtiles_d_));
+    if (aux_ctiles_d_) dev_free(aux_ctiles_d_);
+    if (aux_vtiles_d_) dev_free(aux_vtiles_d_);
     aux_ctiles_d_ = aux_vtiles_d_ = nullptr;
-    DMM_CUDA(cudaMalloc(&aux_ctiles_d_, need * sizeof(Tile)));
-    DMM_CUDA(cudaMalloc(&aux_vtiles_d_, need * sizeof(Tile)));
+    DMM_CUDA(dev_alloc(&aux_ctiles_d_, need * sizeof(Tile)));
+    DMM_CUDA(dev_alloc(&aux_vtiles_d_, need * sizeof(Tile)));
     aux_cap_ = need;
   }
   if (!ct.empty())

@@ -102,6 +102,7 @@ SIGNATURES = {
     "dmm_last_error": (ctypes.c_char_p, []),
     "dmm_params_default": (None, [_P(Params)]),
     "dmm_device_count": (_i32, []),
+    "dmm_release_cached_memory": (None, []),
     "dmm_cnf_read": (_i32, [ctypes.c_char_p, _P(_P(Cnf))]),
     "dmm_cnf_from_arrays": (_i32, [_pi32, _pi64, _i32, _i32, _P(_P(Cnf))]),
     "dmm_cnf_free": (None, [_P(Cnf)]),

@@ -136,6 +136,12 @@ const char* dmm_last_error(void);
 void dmm_params_default(dmm_params* p);
 /* Number of CUDA devices usable by this build (0 when none). */
 int32_t dmm_device_count(void);
+/* No counterpart in the reference.  Instances and batches take their device buffers from a
+ * process-wide cache: a destroyed instance's buffers are kept (up to 8 GiB per device) and
+ * reused by the next instance of a similar size, so that creating and destroying instances
+ * does not go through cudaMalloc/cudaFree (which synchronize the device).  This call returns
+ * every cached block to the driver; live instances keep theirs. */
+void dmm_release_cached_memory(void);
 
 /* ---- formulas (host) ----------------------------------------------------------------- */
 /* DIMACS loader: replaces the parser in main(), dynex.cc:2306-2392 (comment lines skipped,
@@ -227,9 +233,10 @@ dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
 /* Benchmark helper: one cooperative launch of nsteps steps with a device timer read by
  * every block at 10 points of each step (start, clause tile loaded, voltages gathered,
  * phase A done, past grid barrier 1, variable tile loaded, contributions gathered, phase B
- * done, past barrier 2, step decision done).  out[20]: out[2k], out[2k+1] = mean and max
+ * done, past barrier 2, step decision done).  out[21]: out[2k], out[2k+1] = mean and max
  * over blocks of the microseconds from point k to point k+1 (point 10: the next step's
- * start), averaged over steps.  DMM_ERR_STATE on the two-kernel launch form. */
+ * start), averaged over steps; out[20] = the SM clock (MHz) over the traced steps.
+ * DMM_ERR_STATE on the two-kernel launch form. */
 dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double* out);
 
 /* ---- right-hand side without device allocation ----------------------------------------- */

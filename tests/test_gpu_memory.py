@@ -1,0 +1,44 @@
+"""Instances take their device buffers from a process-wide cache (a destroyed instance's
+buffers are reused by the next one).  A reused buffer holds the previous owner's data, so
+these tests check that results never depend on where an instance's memory came from."""
+import numpy as np
+import pytest
+
+import dmm_b200 as dmm
+from dmm_b200._lib import lib
+
+pytestmark = pytest.mark.gpu
+
+
+def run(form, x0, prec, steps):
+    with dmm.Instance(form, precision=prec) as inst:
+        inst.set_state(x0)
+        r = inst.step(steps)
+        x, t = inst.get_state()
+        _, post = inst.assignment(pre=False)
+        return (r.status, r.steps, r.t, r.loc, r.energy), x, post
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_results_do_not_depend_on_reused_memory(prec):
+    form, _ = dmm.generate_planted(20_000, 80_000, 0.08, 0.46, seed=7)
+    other, _ = dmm.generate_planted(20_000, 84_000, 0.08, 0.46, seed=8)
+    x0 = dmm.initial_state_uniform(form, 11)
+    x_other = dmm.initial_state_uniform(other, 12)
+    lib().dmm_release_cached_memory()
+    fresh = run(form, x0, prec, 40)  # buffers straight from the driver
+    for _ in range(2):  # fill the cache with another formula's data, then reuse it
+        run(other, x_other, prec, 40)
+        again = run(form, x0, prec, 40)
+        assert again[0] == fresh[0]
+        assert np.array_equal(again[1], fresh[1])
+        assert np.array_equal(again[2], fresh[2])
+
+
+def test_release_between_instances():
+    form, _ = dmm.generate_planted(5_000, 21_000, 0.08, 0.46, seed=3)
+    x0 = dmm.initial_state_uniform(form, 4)
+    a = run(form, x0, "fp32", 25)
+    lib().dmm_release_cached_memory()
+    b = run(form, x0, "fp32", 25)
+    assert a[0] == b[0] and np.array_equal(a[1], b[1])
