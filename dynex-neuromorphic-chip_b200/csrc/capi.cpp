@@ -99,8 +99,7 @@ dmm_status dmm_instance_create(const int32_t* lits, const int64_t* clause_off, i
   dmm::clear_error();
   if (!out || (precision != DMM_FP32 && precision != DMM_FP64)) return DMM_ERR_ARG;
   *out = nullptr;
-  bool k3;
-  DMM_TRY(dmm::validate_formula(lits, clause_off, n, m, &k3));
+  DMM_TRY(dmm::validate_shape(lits, clause_off, n, m));  // the rest is checked by add()
   auto* inst = new (std::nothrow) dmm_instance();
   if (!inst) return DMM_ERR_NOMEM;
   inst->pack.reset(new (std::nothrow) Pack(precision, device));

@@ -37,9 +37,12 @@ const char* last_error();
   } while (0)
 
 // Validates a formula given as flat literals + offsets.  Sets *k3 when every clause has
-// exactly three literals.
+// exactly three literals, and *may_have_units (if given) unless every clause has two or more.
 dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n,
-                            int32_t m, bool* k3);
+                            int32_t m, bool* k3, bool* may_have_units = nullptr);
+// The checks of validate_formula that do not read the clauses or literals (shape of the
+// arrays and the slot count); the rest is checked when the formula is added to a pack.
+dmm_status validate_shape(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m);
 
 // First-fit allocator of aligned ranges in [0, cap).
 class RangeAlloc {
@@ -177,6 +180,7 @@ class Pack {
   int32_t* vslot_ = nullptr;
   int32_t* upos_ = nullptr;  // variable-major position of each slot
   // staged form (single FP32 formula of 3-literal clauses on the cooperative path)
+  std::vector<int8_t> unit_h_;  // unit pins of the formula being added
   bool xp_active_ = false;
   bool one_active_ = false;  // single FP32 formula on the cooperative path
   enum { kXpDlist, kXpDoff, kXpLlit, kXpSpos, kXpUx, kXpUbase, kXpBoff, kXpSrc8, kXpDst,

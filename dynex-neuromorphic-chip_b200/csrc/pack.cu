@@ -27,8 +27,7 @@ void set_error(const char* fmt, ...) {
 void clear_error() { g_err.clear(); }
 const char* last_error() { return g_err.c_str(); }
 
-dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
-                            bool* k3) {
+dmm_status validate_shape(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m) {
   if (n <= 0 || m < 0 || clause_off == nullptr) {
     set_error("formula: need n > 0, m >= 0 and clause offsets");
     return DMM_ERR_ARG;
@@ -37,18 +36,47 @@ dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int3
     set_error("formula: clause_off[0] must be 0");
     return DMM_ERR_ARG;
   }
-  bool all3 = m > 0;
+  const int64_t L = clause_off[m];
+  if (L < 0 || L > 0x7fffffffll - 64) {
+    set_error("formula: %lld literals outside the 2^31 slot limit", (long long)L);
+    return DMM_ERR_ARG;
+  }
+  if (L > 0 && lits == nullptr) {
+    set_error("formula: literals missing");
+    return DMM_ERR_ARG;
+  }
+  return DMM_OK;
+}
+
+dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
+                            bool* k3, bool* may_have_units) {
+  if (n <= 0 || m < 0 || clause_off == nullptr) {
+    set_error("formula: need n > 0, m >= 0 and clause offsets");
+    return DMM_ERR_ARG;
+  }
+  if (clause_off[0] != 0) {
+    set_error("formula: clause_off[0] must be 0");
+    return DMM_ERR_ARG;
+  }
+  // branch-free passes (they vectorize); the slow loops below only locate an error
+  int64_t lmin = INT64_MAX, lmax = INT64_MIN;
   for (int32_t c = 0; c < m; c++) {
     const int64_t len = clause_off[c + 1] - clause_off[c];
-    if (len < 0) {
-      set_error("formula: clause offsets decrease at clause %d", c);
-      return DMM_ERR_ARG;
+    lmin = len < lmin ? len : lmin;
+    lmax = len > lmax ? len : lmax;
+  }
+  if (m > 0 && (lmin < 0 || lmax > DMM_MAX_CLAUSE_LITS)) {
+    for (int32_t c = 0; c < m; c++) {
+      const int64_t len = clause_off[c + 1] - clause_off[c];
+      if (len < 0) {
+        set_error("formula: clause offsets decrease at clause %d", c);
+        return DMM_ERR_ARG;
+      }
+      if (len > DMM_MAX_CLAUSE_LITS) {
+        set_error("CLAUSE %d HAS MORE THAN %d LITERALS", c, DMM_MAX_CLAUSE_LITS);
+        return DMM_ERR_CLAUSE_LEN;
+      }
     }
-    if (len > DMM_MAX_CLAUSE_LITS) {
-      set_error("CLAUSE %d HAS MORE THAN %d LITERALS", c, DMM_MAX_CLAUSE_LITS);
-      return DMM_ERR_CLAUSE_LEN;
-    }
-    if (len != 3) all3 = false;
   }
   const int64_t L = clause_off[m];
   if (L > 0x7fffffffll - 64) {
@@ -59,14 +87,25 @@ dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int3
     set_error("formula: literals missing");
     return DMM_ERR_ARG;
   }
+  // -n <= l <= n, l != 0: (unsigned)l + n lies in [0, 2n]
+  const uint32_t un = (uint32_t)n, span = 2u * (uint32_t)n;
+  uint32_t bad = 0;
   for (int64_t s = 0; s < L; s++) {
     const int32_t l = lits[s];
-    if (l == 0 || l > n || l < -n) {
-      set_error("formula: literal %d at position %lld out of range for n=%d", l, (long long)s, n);
-      return DMM_ERR_LITERAL;
+    bad |= (uint32_t)(l == 0) | (uint32_t)((uint32_t)l + un > span);
+  }
+  if (bad) {
+    for (int64_t s = 0; s < L; s++) {
+      const int32_t l = lits[s];
+      if (l == 0 || l > n || l < -n) {
+        set_error("formula: literal %d at position %lld out of range for n=%d", l, (long long)s,
+                  n);
+        return DMM_ERR_LITERAL;
+      }
     }
   }
-  *k3 = all3;
+  *k3 = m > 0 && lmin == 3 && lmax == 3;
+  if (may_have_units) *may_have_units = m > 0 && lmin <= 1;
   return DMM_OK;
 }
 
@@ -445,8 +484,8 @@ static dmm_status upload_alpha(T* dst, const double* a, int32_t m, cudaStream_t 
 dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
                      const dmm_params* p, const double* alpha_cm, int32_t max_steps,
                      int32_t* idx_out) {
-  bool k3 = false;
-  DMM_TRY(validate_formula(lits, clause_off, n, m, &k3));
+  bool k3 = false, units = true;
+  DMM_TRY(validate_formula(lits, clause_off, n, m, &k3, &units));
   if (alpha_cm && !with_alpha_cm_) {
     set_error("this pack was created without per-clause alpha storage");
     return DMM_ERR_ARG;
@@ -493,13 +532,17 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
                              cudaMemcpyHostToDevice, stream_));
   }
   // unit clauses (dynex.cc:2459-2469: the last unit clause of a variable wins)
-  std::vector<int8_t> unit(n, 0);
-  for (int32_t c = 0; c < m; c++)
-    if (clause_off[c + 1] - clause_off[c] == 1) {
-      const int32_t l = lits[clause_off[c]];
-      unit[std::abs(l) - 1] = l > 0 ? 1 : -1;
-    }
-  DMM_CUDA(cudaMemcpyAsync(unit_ + var0, unit.data(), n, cudaMemcpyHostToDevice, stream_));
+  if (units) {
+    unit_h_.assign(n, 0);
+    for (int32_t c = 0; c < m; c++)
+      if (clause_off[c + 1] - clause_off[c] == 1) {
+        const int32_t l = lits[clause_off[c]];
+        unit_h_[std::abs(l) - 1] = l > 0 ? 1 : -1;
+      }
+    DMM_CUDA(cudaMemcpyAsync(unit_ + var0, unit_h_.data(), n, cudaMemcpyHostToDevice, stream_));
+  } else {
+    DMM_CUDA(cudaMemsetAsync(unit_ + var0, 0, n, stream_));
+  }
   if (alpha_cm) {
     if (prec_ == DMM_FP64)
       DMM_TRY(upload_alpha(static_cast<double*>(alpha_cm_) + cls0, alpha_cm, m, stream_));

@@ -42,3 +42,24 @@ def test_release_between_instances():
     lib().dmm_release_cached_memory()
     b = run(form, x0, "fp32", 25)
     assert a[0] == b[0] and np.array_equal(a[1], b[1])
+
+
+def test_instance_rejects_bad_formulas():
+    """Creation rejects bad literals and clause lengths with DMM_ERR_LITERAL, _CLAUSE_LEN and
+    _ARG, and the library keeps working after the rejections."""
+    def make(lits, off, n):
+        return dmm.Formula(n, len(off) - 1, np.asarray(lits, np.int32),
+                           np.asarray(off, np.int64), 1)
+    cases = [(make([1, -2, 5], [0, 3], 3), "DMM_ERR_LITERAL"),
+             (make([1, 0, 2], [0, 3], 3), "DMM_ERR_LITERAL"),
+             (make(list(range(1, 27)), [0, 26], 30), "DMM_ERR_CLAUSE_LEN"),
+             (make([1, 2, 3], [0, 3, 2], 3), "DMM_ERR_ARG")]
+    for form, name in cases:
+        for prec in ("fp32", "fp64"):
+            with pytest.raises(dmm.DmmError) as e:
+                dmm.Instance(form, precision=prec)
+            assert e.value.name == name
+    ok, _ = dmm.generate_planted(1_000, 4_200, 0.08, 0.46, seed=5)
+    with dmm.Instance(ok, precision="fp32") as inst:
+        inst.set_state(dmm.initial_state_uniform(ok, 6))
+        assert inst.step(3).steps == 3
