@@ -168,10 +168,16 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+KERNELS = {"staged": "k_staged (fused step, staged form)",
+           "cooperative-single": "k_persist (fused step, single formula)",
+           "cooperative": "k_persist (fused step)",
+           "two-kernel": "k_clause + k_var", "one-block-per-formula": "k_inst"}
+
+
 def profiled_traffic() -> float | None:
-    """DRAM bytes per launch of the clause kernel at this workload, from the committed
-    ncu summary (profiles/k_persist_n100k.md, line `traffic_bytes_per_launch: X`)."""
-    p = os.path.join(ROOT, "profiles", "k_persist_n100k.md")
+    """DRAM bytes per launch of the step kernel at this workload, from the committed ncu
+    summary (profiles/k_staged_n100k.md, line `traffic_bytes_per_launch: X`)."""
+    p = os.path.join(ROOT, "profiles", "k_staged_n100k.md")
     try:
         with open(p) as f:
             m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
@@ -298,6 +304,7 @@ def main():
     n, m = form.n, form.m
     K, W = a.steps, max(3, a.warmup)
     inst = dmm.Instance(form, precision="fp32", device=local)
+    form_name = inst.launch_form
     init_seed = INIT_SEED + rank
     for attempt in range(4):
         inst.set_state(x0)
@@ -390,7 +397,7 @@ def main():
             "gpu_launches": K,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_persist (fused step)", "peak_kind": peak_kind,
+                         "kernel": KERNELS[form_name], "peak_kind": peak_kind,
                          "algo_bytes_per_launch": algo_bytes},
             "phase_ms_per_step": {"k_clause": clause_ms / K, "k_var": var_ms / K,
                                   "note": "kernel-per-phase form, L2 flushed"},

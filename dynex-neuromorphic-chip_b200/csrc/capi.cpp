@@ -260,6 +260,11 @@ dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
   return inst->pack->time_steps_flushed(nsteps, flush_bytes, ms);
 }
 
+int32_t dmm_instance_launch_form(const dmm_instance* inst) {
+  if (!inst) return DMM_ERR_ARG;
+  return inst->pack->launch_form();
+}
+
 dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double* out) {
   dmm::clear_error();
   if (!inst || nsteps <= 0 || !out) return DMM_ERR_ARG;

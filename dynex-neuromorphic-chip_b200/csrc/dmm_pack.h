@@ -113,6 +113,9 @@ class Pack {
   // point k to point k+1 (point kTraceK: the next step's start), averaged over steps;
   // out[2 kTraceK] = SM clock (MHz).
   dmm_status trace_phases(int32_t nsteps, double* out);
+  // Kernel used by launch_steps: 1 two-kernel, 2 cooperative, 3 cooperative single formula,
+  // 4 staged, 5 one block per formula (dmm_instance_launch_form).
+  int launch_form() const;
   // Raises DMM_ERR_CUDA when a cooperative launch reported a grid-barrier timeout.
   dmm_status check_error();
   dmm_status read_active(int32_t* active);
@@ -182,7 +185,8 @@ class Pack {
   // staged form (single FP32 formula of 3-literal clauses on the cooperative path)
   std::vector<int8_t> unit_h_;  // unit pins of the formula being added
   bool xp_active_ = false;
-  bool one_active_ = false;  // single FP32 formula on the cooperative path
+  bool one_active_ = false;
+  bool launch_area_clean_ = false;  // cooperative launch area zeroed (see leave_launch)  // single FP32 formula on the cooperative path
   enum { kXpDlist, kXpDoff, kXpLlit, kXpSpos, kXpUx, kXpUbase, kXpBoff, kXpSrc8, kXpDst,
          kXpScratch, kXpBufs };
   void* xbuf_[kXpBufs] = {};

@@ -525,6 +525,27 @@ __device__ __forceinline__ void load_tile_one(TileSmem<NT>& sm, const LocalSnap&
   __syncthreads();
 }
 
+// Number of ints at `bar` that a cooperative launch uses (barrier counter, exit counter,
+// the StepAcc pair) and leaves zeroed for the next launch.
+constexpr int kLaunchAreaInts = 32;
+
+// Called by every block of a cooperative launch that did not give up at a barrier, after its
+// last read of the launch area: the last block to leave zeroes the area (the barrier
+// counter, this exit counter at bar[1], the step accumulators), so that the next launch on
+// the stream starts from zero without a separate memset.
+__device__ __forceinline__ void leave_launch(unsigned int* bar) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(bar + 1, 1u);
+    if (prev == gridDim.x - 1) {
+      volatile unsigned int* a = bar;
+      for (int i = 0; i < kLaunchAreaInts; i++) a[i] = 0u;
+      __threadfence();
+    }
+  }
+}
+
 // nsteps integration steps in one cooperative launch.  Blocks own tiles statically
 // (tile ti -> block ti % gridDim.x); phases A | B | F are separated by grid barriers.
 // ONE (a single FP32 formula): two grid barriers per step.  The step's counts go to the
@@ -634,6 +655,7 @@ __global__ void __launch_bounds__(NT, 1)
       if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
     }
   }
+  leave_launch(bar);
 }
 
 }  // namespace dmm

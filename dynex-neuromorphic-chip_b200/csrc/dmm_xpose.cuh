@@ -486,6 +486,7 @@ __global__ void __launch_bounds__(NT, 1)
     if (!s_ok) return;
     trace_stamp(P, s, 9);
   }
+  leave_launch(bar);
 }
 
 }  // namespace dmm

@@ -1036,9 +1036,14 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
     view = &vf;
   }
   static_assert(kMiscAcc2 * 4 + 2 * sizeof(StepAcc) <= kMiscInts * 4, "misc area");
+  static_assert(kMiscInts - kMiscLaunch == kLaunchAreaInts, "launch area");
   unsigned int* bar = reinterpret_cast<unsigned int*>(misc_d_ + kMiscLaunch);
   int* err = misc_d_ + 1;
-  DMM_CUDA(cudaMemsetAsync(bar, 0, (kMiscInts - kMiscLaunch) * sizeof(int32_t), stream_));
+  // a completed launch leaves its area zeroed (leave_launch); after an error or before the
+  // first launch it is zeroed here
+  if (!launch_area_clean_)
+    DMM_CUDA(cudaMemsetAsync(bar, 0, kLaunchAreaInts * sizeof(int32_t), stream_));
+  launch_area_clean_ = true;
   void* args[] = {view, &nsteps, &bar, &err};
   const size_t smem = xp_active_ ? (size_t)xsmem_ : 0;
   if (smem)
@@ -1086,6 +1091,7 @@ dmm_status Pack::check_error() {
   DMM_CUDA(cudaMemcpyAsync(&e, misc_d_ + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
   DMM_CUDA(cudaStreamSynchronize(stream_));
   if (e) {
+    launch_area_clean_ = false;
     set_error("grid barrier wait gave up in the cooperative step kernel");
     return DMM_ERR_CUDA;
   }
@@ -1169,6 +1175,14 @@ dmm_status Pack::time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double*
   }
   *ms = total;
   return check_error();
+}
+
+int Pack::launch_form() const {
+  if (tun_.launch_mode == 1) return 1;
+  if (ctiles_h_.empty() && vtiles_h_.empty() && n_small_ > 0) return 5;
+  if (xp_active_) return 4;
+  if (one_active_) return 3;
+  return 2;
 }
 
 dmm_status Pack::trace_phases(int32_t nsteps, double* out) {

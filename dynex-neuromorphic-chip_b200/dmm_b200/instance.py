@@ -184,6 +184,17 @@ class Instance:
                                                     ctypes.byref(ms)))
         return ms.value
 
+    LAUNCH_FORMS = {1: "two-kernel", 2: "cooperative", 3: "cooperative-single",
+                    4: "staged", 5: "one-block-per-formula"}
+
+    @property
+    def launch_form(self) -> str:
+        """Kernel that step/solve launch with the current tuning (see LAUNCH_FORMS)."""
+        f = lib().dmm_instance_launch_form(self._h)
+        if f < 0:
+            check(f)
+        return self.LAUNCH_FORMS[f]
+
     def trace_phases(self, nsteps: int) -> dict:
         """Per-step microseconds (mean, max over blocks) between the cooperative kernel's
         trace points, averaged over one launch of nsteps steps."""

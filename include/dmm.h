@@ -217,6 +217,15 @@ dmm_status dmm_instance_report(dmm_instance* inst, dmm_report* rep);
  *        of dynex.cc:667-670 and the solution file of dynex.cc:693-699),
  *  post: the reported assignment after the final step (+1/-1; `v` lines, dynex.cc:1506-1512). */
 dmm_status dmm_instance_assignment(dmm_instance* inst, int8_t* pre, int8_t* post);
+/* No counterpart in the reference.  The kernel that dmm_instance_step / _solve launch for
+ * this instance with its current tuning:
+ *   1  two kernels per step (clause tiles, then variable tiles), CUDA graphs
+ *   2  one cooperative kernel for several steps, three grid barriers per step
+ *   3  the same for a single FP32 formula: two grid barriers per step
+ *   4  the staged single-formula kernel (FP32, 3-literal clauses, tables fit)
+ *   5  one block per formula
+ * or a negative dmm_status. */
+int32_t dmm_instance_launch_form(const dmm_instance* inst);
 /* Benchmark helper: runs nsteps steps as plain launches with CUDA events around each of
  * the two step kernels; before each step it writes flush_bytes of scratch (0: none) so
  * the step starts with a cold L2.  Returns the summed device times (ms). */

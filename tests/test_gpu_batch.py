@@ -134,6 +134,7 @@ def test_full_size_fp32_bitexact_vs_oracle_first_steps(big):
     o = Oracle(form.n, form.m, form.lits, form.clause_off, precision="fp32")
     ref = o.run(x0, 12, dump_every=4)
     with dmm.Instance(form, precision="fp32") as inst:
+        assert inst.launch_form == "staged"  # the production kernel at this size
         inst.set_state(x0)
         for r in range(1, 4):
             inst.step(4)

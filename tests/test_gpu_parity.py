@@ -135,6 +135,7 @@ def test_fp32_per_step_bitexact_vs_oracle_fp32(fixtures, name, seed):
     x0 = uniform_init(f["n"], f["m"], seed)
     ref = o.run(x0, 400, dump_every=1)
     with dmm.Instance(formula(f), precision="fp32") as inst:
+        assert inst.launch_form == "staged"
         rows, rep = run_steps(inst, x0, 400)
     assert rep.steps == ref["steps"]
     assert np.array_equal(rows, ref["dump"][: ref["steps"] + 1])
@@ -149,12 +150,15 @@ def test_fp32_launch_shape_does_not_change_results(fixtures):
                                        (4, 32, 0, 0, 0), (8, 64, 4096, 1024, 1),
                                        (16, 3, 256, 32, 0), (32, 256, 8192, 256, 1),
                                        (4, 5, 260, 96, 2), (8, 9, 0, 0, 3), (1, 40, 0, 0, 3)]]
+    forms = set()
     for kw in shapes:
         with dmm.Instance(formula(f), precision="fp32") as inst:
             inst.set_tuning(**kw)
+            forms.add(inst.launch_form)
             inst.set_state(x0)
             inst.step(150)
             outs.append((inst.get_state()[0], inst.report().steps))
+    assert forms == {"staged", "cooperative-single", "two-kernel", "one-block-per-formula"}
     for x, s in outs[1:]:
         assert s == outs[0][1]
         assert np.array_equal(x, outs[0][0])
@@ -172,6 +176,10 @@ def test_contribution_layout_does_not_change_results(fixtures, prec):
             continue
         with dmm.Instance(formula(f), precision=prec) as inst:
             inst.set_tuning(u_layout=lay, launch_mode=mode)
+            if mode == 0:  # the staged kernel is the FP32 default layout's
+                want = "staged" if prec == "fp32" and lay == 0 else (
+                    "cooperative-single" if prec == "fp32" else "cooperative")
+                assert inst.launch_form == want
             inst.set_state(x0)
             inst.step(120)
             d, loc, _ = inst.generate_dxdt(inst.get_state()[0])
