@@ -215,17 +215,10 @@ __device__ __forceinline__ T tree_sum(const T* u, const Idx* __restrict__ vs,
 // Reference summation (dynex.cc:527-530): contributions sorted ascending, summed left to
 // right from +0.0 (zero contributions, which the reference skips, change no partial sum).
 // One warp per variable; d must be warp-uniform.  Bitonic sort in registers for d <= 32R.
-template <int R, bool DIRECT, class Idx>
-__device__ __forceinline__ double sorted_sum_reg(const double* u,
-                                                 const Idx* __restrict__ vs, int d,
-                                                 int lane) {
-  double a[R];
-  const double pinf = inf_val<double>();
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    const int j = r * 32 + lane;
-    a[r] = (j < d) ? (DIRECT ? u[j] : u[__ldg(vs + j)]) : pinf;
-  }
+// Sorts the 32R values a[r] of lane `lane` (entry r * 32 + lane; +inf beyond d) across the
+// warp and returns the left-to-right sum of the d smallest.
+template <int R>
+__device__ __forceinline__ double sort_sum_vals(double (&a)[R], int d, int lane) {
   constexpr int N = 32 * R;
 #pragma unroll
   for (int k = 2; k <= N; k <<= 1) {
@@ -269,6 +262,20 @@ __device__ __forceinline__ double sorted_sum_reg(const double* u,
     }
   }
   return acc;
+}
+
+template <int R, bool DIRECT, class Idx>
+__device__ __forceinline__ double sorted_sum_reg(const double* u,
+                                                 const Idx* __restrict__ vs, int d,
+                                                 int lane) {
+  double a[R];
+  const double pinf = inf_val<double>();
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int j = r * 32 + lane;
+    a[r] = (j < d) ? (DIRECT ? u[j] : u[__ldg(vs + j)]) : pinf;
+  }
+  return sort_sum_vals<R>(a, d, lane);
 }
 
 // Long lists: repeated selection of the next (value, position) pair in lexicographic

@@ -116,6 +116,9 @@ class Pack {
   // Kernel used by launch_steps: 1 two-kernel, 2 cooperative, 3 cooperative single formula,
   // 4 staged, 5 one block per formula (dmm_instance_launch_form).
   int launch_form() const;
+  // Loads every kernel this pack's precision and tuning can launch (the driver otherwise
+  // loads a kernel at its first launch, which would stall a running service).
+  dmm_status preload_kernels();
   // Raises DMM_ERR_CUDA when a cooperative launch reported a grid-barrier timeout.
   dmm_status check_error();
   dmm_status read_active(int32_t* active);

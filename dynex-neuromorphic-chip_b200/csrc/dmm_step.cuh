@@ -273,6 +273,106 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
   const int grp = threadIdx.x / G, lane = threadIdx.x % G;
   const int v_end = sm.tile.begin + sm.tile.count;
   int kmax = 0;
+  // candidates and trial index of variable v from its sum dv (lane 0 of its group)
+  auto finish = [&](int v, T dv) {
+    if (MODE == 1) {
+      dv_out[v] = (double)dv;
+    } else {
+      const T V = cur[v];
+      const int8_t un = unit[v];
+      int kv = kTrials;
+#pragma unroll
+      for (int k = 0; k < kTrials; k++) {
+        const T h = T(0.125 / (double)(1 << k));
+        T c = add(V, mul(h, dv));
+        if (un != 0) c = T(un);
+        c = clampv(c, T(-1), T(1));
+        nxt[(int64_t)k * P.var_cap + v] = c;
+        const bool fail = fabs((double)c - (double)V) >= 1.0;
+        if (!fail && kv == kTrials) kv = k;
+      }
+      kmax = max(kmax, kv);
+    }
+  };
+  if constexpr (SORTED) {
+    // FP64 reference sums: four variables per warp, eight lanes each holding four entries
+    // (entry e = lane-in-segment + 8 r); one bitonic network sorts the four lists at once
+    // and the ascending left-to-right sum takes one shuffle per entry position for all four.
+    // Lists longer than 32 take the warp-wide sum afterwards.
+    static_assert(G == 32, "the sorted sum is organized per warp");
+    constexpr int SEG = 8, NV = 32 / SEG, RR = 4;
+    const double* ud = reinterpret_cast<const double*>(u);
+    const double pinf = inf_val<double>();
+    const int seg = lane / SEG, sl = lane % SEG;
+    for (int vb = sm.tile.begin + grp * NV; vb < v_end; vb += VPP * NV) {
+      const int v = vb + seg;
+      const bool valid = v < v_end;
+      int s0 = 0, d = 0;
+      if (valid) {
+        const int s1 = __ldg(vend + v);
+        s0 = v > 0 ? __ldg(vend + v - 1) : 0;
+        d = s1 - s0;
+      }
+      const bool small = valid && d <= SEG * RR;
+      double a[RR];
+#pragma unroll
+      for (int r = 0; r < RR; r++) {
+        const int e = sl + SEG * r;
+        a[r] = (small && e < d) ? (P.upos ? ud[s0 + e] : ud[__ldg(vsl + s0 + e)]) : pinf;
+      }
+#pragma unroll
+      for (int k = 2; k <= SEG * RR; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          if (j >= SEG) {  // partner in another register of the same lane
+            const int jr = j / SEG;
+#pragma unroll
+            for (int r = 0; r < RR; r++) {
+              const int r2 = r ^ jr;
+              if (r2 > r) {
+                const bool up = ((sl + SEG * r) & k) == 0;
+                const double x = a[r], y = a[r2];
+                const bool sw = up ? (y < x) : (x < y);
+                a[r] = sw ? y : x;
+                a[r2] = sw ? x : y;
+              }
+            }
+          } else {  // partner lane sl ^ j of the same segment
+#pragma unroll
+            for (int r = 0; r < RR; r++) {
+              const int e = sl + SEG * r;
+              const double o = __shfl_xor_sync(0xffffffffu, a[r], j);
+              const bool up = (e & k) == 0;
+              const bool lower = (e & j) == 0;
+              const double mn = (o < a[r]) ? o : a[r];
+              const double mx = (o < a[r]) ? a[r] : o;
+              a[r] = (lower == up) ? mn : mx;
+            }
+          }
+        }
+      }
+      double acc = 0.0;
+#pragma unroll
+      for (int r = 0; r < RR; r++) {
+#pragma unroll
+        for (int l = 0; l < SEG; l++) {
+          const double x = __shfl_sync(0xffffffffu, a[r], seg * SEG + l);
+          if (SEG * r + l < d) acc = __dadd_rn(acc, x);
+        }
+      }
+      if (small && sl == 0) finish(v, T(acc));
+      unsigned long_lists = __ballot_sync(0xffffffffu, valid && !small && sl == 0);
+      while (long_lists) {  // warp-uniform
+        const int sg = (__ffs(long_lists) - 1) / SEG;
+        long_lists &= long_lists - 1;
+        const int vl = vb + sg;
+        const int e1 = __ldg(vend + vl), e0 = vl > 0 ? __ldg(vend + vl - 1) : 0;
+        const double dv = P.upos ? sorted_sum<true, int32_t>(ud + e0, nullptr, e1 - e0, lane)
+                                 : sorted_sum<false>(ud, vsl + e0, e1 - e0, lane);
+        if (lane == 0) finish(vl, T(dv));
+      }
+    }
+  } else {
   for (int vb = sm.tile.begin; vb < v_end; vb += VPP) {
     const int v = vb + grp;
     const bool valid = v < v_end;
@@ -281,35 +381,10 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
       s1 = __ldg(vend + v);
       s0 = v > 0 ? __ldg(vend + v - 1) : 0;
     }
-    T dv;
-    if constexpr (SORTED) {
-      const double* ud = reinterpret_cast<const double*>(u);
-      dv = P.upos ? T(sorted_sum<true, int32_t>(ud + s0, nullptr, s1 - s0, lane))
-                  : T(sorted_sum<false>(ud, vsl + s0, s1 - s0, lane));
-    } else {
-      dv = P.upos ? tree_sum<T, G, true, int32_t>(u + s0, nullptr, s1 - s0, lane)
-                  : tree_sum<T, G, false>(u, vsl + s0, s1 - s0, lane);
-    }
-    if (valid && lane == 0) {
-      if (MODE == 1) {
-        dv_out[v] = (double)dv;
-      } else {
-        const T V = cur[v];
-        const int8_t un = unit[v];
-        int kv = kTrials;
-#pragma unroll
-        for (int k = 0; k < kTrials; k++) {
-          const T h = T(0.125 / (double)(1 << k));
-          T c = add(V, mul(h, dv));
-          if (un != 0) c = T(un);
-          c = clampv(c, T(-1), T(1));
-          nxt[(int64_t)k * P.var_cap + v] = c;
-          const bool fail = fabs((double)c - (double)V) >= 1.0;
-          if (!fail && kv == kTrials) kv = k;
-        }
-        kmax = max(kmax, kv);
-      }
-    }
+    const T dv = P.upos ? tree_sum<T, G, true, int32_t>(u + s0, nullptr, s1 - s0, lane)
+                        : tree_sum<T, G, false>(u, vsl + s0, s1 - s0, lane);
+    if (valid && lane == 0) finish(v, dv);
+  }
   }
   if (MODE == 0) {
     kmax = warp_max_i(kmax);

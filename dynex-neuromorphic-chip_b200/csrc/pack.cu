@@ -175,7 +175,8 @@ int64_t Pack::bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
   n = RangeAlloc::round(std::max<int64_t>(n, 1));
   m = RangeAlloc::round(std::max<int64_t>(m, 1));
   slots = RangeAlloc::round(std::max<int64_t>(slots, 1));
-  int64_t b = m * (3 * t + 4 + (with_alpha_cm ? t : 0)) + slots * (8 + t) + n * (8 * t + 9);
+  // per slot: literal, CSR entry, variable-major position (4 each) and the contribution
+  int64_t b = m * (3 * t + 4 + (with_alpha_cm ? t : 0)) + slots * (12 + t) + n * (8 * t + 9);
   b += (m / kMinClauseTile + 1) * (8 + 16) + (n / kMinVarTile + 1) * 16;
   b += sizeof(InstDesc) + sizeof(InstCtrl) + 8;
   return b;
@@ -1175,6 +1176,40 @@ dmm_status Pack::time_steps_flushed(int32_t nsteps, int64_t flush_bytes, double*
   }
   *ms = total;
   return check_error();
+}
+
+dmm_status Pack::preload_kernels() {
+  DMM_CUDA(cudaSetDevice(dev_));
+  const int G = tun_.var_group;
+  std::vector<const void*> fns = {
+      persist_fn_x<false>(prec_, G), (const void*)k_count, (const void*)k_scan_block,
+      (const void*)k_scan_add, (const void*)k_fill_start, (const void*)k_scatter,
+      (const void*)k_sort_lists, (const void*)k_invert, (const void*)k_active_add};
+  if (prec_ == DMM_FP64) {
+    fns.push_back((const void*)k_set_state<double>);
+    fns.push_back((const void*)k_get_state<double>);
+  } else {
+    fns.push_back((const void*)k_set_state<float>);
+    fns.push_back((const void*)k_get_state<float>);
+    fns.push_back(persist_fn_x<true>(prec_, G));
+    fns.push_back(staged_fn(G));
+    fns.push_back((const void*)k_xp_count<kXprepThreads>);
+    fns.push_back((const void*)k_xp_scan<kXprepThreads>);
+    fns.push_back((const void*)k_xp_fill<kXprepThreads>);
+    switch (G) {
+      case 1: fns.push_back((const void*)k_inst<1>); break;
+      case 2: fns.push_back((const void*)k_inst<2>); break;
+      case 4: fns.push_back((const void*)k_inst<4>); break;
+      case 8: fns.push_back((const void*)k_inst<8>); break;
+      case 16: fns.push_back((const void*)k_inst<16>); break;
+      default: fns.push_back((const void*)k_inst<32>); break;
+    }
+  }
+  for (const void* f : fns) {
+    cudaFuncAttributes a;
+    DMM_CUDA(cudaFuncGetAttributes(&a, f));
+  }
+  return DMM_OK;
 }
 
 int Pack::launch_form() const {

@@ -69,9 +69,10 @@ dmm_status dmm_server_create(const dmm_server_config* cfg, dmm_server** out) {
   if (s->cfg.steps_per_launch <= 0) s->cfg.steps_per_launch = 32;
   s->pack.reset(new (std::nothrow) Pack((dmm_precision)cfg->precision, cfg->device));
   // Arena capacities from the budget: a 3-literal clause costs 3t+4 bytes plus 3 slots of
-  // 8+t; variables get a quarter of the budget so formulas down to ratio ~2 fit.
+  // 12+t (Pack::bytes_per); variables get a quarter of the budget so formulas down to ratio
+  // ~2 fit.
   const int64_t t = cfg->precision == DMM_FP64 ? 8 : 4;
-  const int64_t per_clause = 3 * t + 4 + 3 * (8 + t);
+  const int64_t per_clause = 3 * t + 4 + 3 * (12 + t);
   const int64_t per_var = 8 * t + 9;
   dmm::PackCaps caps;
   caps.insts = cfg->max_slots;
@@ -86,6 +87,7 @@ dmm_status dmm_server_create(const dmm_server_config* cfg, dmm_server** out) {
   dmm_tuning tun{};
   tun.steps_per_graph = s->cfg.steps_per_launch;
   st = s->pack->set_tuning(&tun);
+  if (st == DMM_OK) st = s->pack->preload_kernels();
   if (st != DMM_OK) {
     delete s;
     return st;
