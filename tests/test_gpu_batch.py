@@ -186,3 +186,23 @@ def test_many_small_formulas_auto_mode_equal_alone(fixtures):
             r_a.status, r_a.steps, r_a.solved_step, r_a.t, r_a.loc)
         assert np.array_equal(b.state(k)[0], x_a)
         assert np.array_equal(post_b, post_a)
+
+
+@pytest.mark.parametrize("n,m,form_want", [(200_000, 840_000, "staged"),
+                                           (300_000, 1_260_000, "cooperative-single")])
+def test_staged_kernel_limits(n, m, form_want):
+    """The staged kernel applies while its tile tables fit (16-bit indices, shared memory);
+    beyond that the instance runs the plain single-formula kernel.  Either way the states
+    equal the plain kernel's bit for bit."""
+    form, _ = dmm.generate_planted(n, m, p0=0.08, p1=0.46, seed=n)
+    x0 = dmm.initial_state_uniform(form, 5)
+    outs = []
+    for lay in (0, 1):
+        with dmm.Instance(form, precision="fp32") as inst:
+            inst.set_tuning(u_layout=lay)
+            assert inst.launch_form == (form_want if lay == 0 else "cooperative-single")
+            inst.set_state(x0)
+            rep = inst.step(10)
+            outs.append((inst.get_state()[0], rep.t, rep.loc, rep.energy))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1:] == outs[1][1:]
