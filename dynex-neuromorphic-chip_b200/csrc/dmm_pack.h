@@ -111,7 +111,8 @@ class Pack {
   // One cooperative launch of nsteps steps with %globaltimer stamps at kTraceK points of
   // every step; out[2k], out[2k+1] = mean and max over blocks of the microseconds from
   // point k to point k+1 (point kTraceK: the next step's start), averaged over steps;
-  // out[2 kTraceK] = SM clock (MHz).
+  // out[2 kTraceK] = SM clock (MHz); out[2 kTraceK + 1], [+ 2] = launch prologue and epilogue
+  // (staged kernel).
   dmm_status trace_phases(int32_t nsteps, double* out);
   // Kernel used by launch_steps: 1 two-kernel, 2 cooperative, 3 cooperative single formula,
   // 4 staged, 5 one block per formula (dmm_instance_launch_form).

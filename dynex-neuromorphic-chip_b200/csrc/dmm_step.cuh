@@ -62,6 +62,17 @@ __device__ __forceinline__ void trace_stamp(const PackView<T>& P, int s, int k) 
   }
 }
 
+// Records %globaltimer at kernel entry (which 0) or exit (which 1) of this block, after
+// the step stamps and clock counts (thread 0; no-op unless tracing).
+template <class T>
+__device__ __forceinline__ void trace_launch(const PackView<T>& P, int which) {
+  if (P.trace && threadIdx.x == 0) {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    P.trace[(int64_t)2 * P.trace_steps * kTraceK * gridDim.x + which * gridDim.x + blockIdx.x] = t;
+  }
+}
+
 struct TileSnap {
   int32_t done, pending, set, kcur;
   double h;

@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(NT, 1)
   const bool has_c = b < nct, has_v = b < nvt;
   const int ii = P.live[0];
 
+  trace_launch(P, 0);
   // ---- launch setup: description, control state, ranges, launch-constant tables
   if (tid == 0) {
     I = P.inst[ii];
@@ -487,6 +488,7 @@ __global__ void __launch_bounds__(NT, 1)
     trace_stamp(P, s, 9);
   }
   leave_launch(bar);
+  trace_launch(P, 1);
 }
 
 }  // namespace dmm

@@ -198,10 +198,12 @@ class Instance:
     def trace_phases(self, nsteps: int) -> dict:
         """Per-step microseconds (mean, max over blocks) between the cooperative kernel's
         trace points, averaged over one launch of nsteps steps."""
-        out = (ctypes.c_double * 21)()
+        out = (ctypes.c_double * 23)()
         check(lib().dmm_instance_trace_phases(self._h, int(nsteps), out))
         keys = ("a_load", "a_gather", "a_eval", "barrier1", "b_load", "b_gather", "b_reduce",
                 "barrier2", "decide", "barrier3")
         r = {k: (out[2 * i], out[2 * i + 1]) for i, k in enumerate(keys)}
         r["sm_mhz"] = out[20]
+        r["launch_prologue"] = out[21]
+        r["launch_epilogue"] = out[22]
         return r

@@ -242,9 +242,11 @@ dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
 /* Benchmark helper: one cooperative launch of nsteps steps with a device timer read by
  * every block at 10 points of each step (start, clause tile loaded, voltages gathered,
  * phase A done, past grid barrier 1, variable tile loaded, contributions gathered, phase B
- * done, past barrier 2, step decision done).  out[21]: out[2k], out[2k+1] = mean and max
+ * done, past barrier 2, step decision done).  out[23]: out[2k], out[2k+1] = mean and max
  * over blocks of the microseconds from point k to point k+1 (point 10: the next step's
- * start), averaged over steps; out[20] = the SM clock (MHz) over the traced steps.
+ * start), averaged over steps; out[20] = the SM clock (MHz) over the traced steps;
+ * out[21], out[22] = mean microseconds from kernel entry to the first step (launch set-up)
+ * and from the last step's end to kernel exit (staged kernel; 0 for the others).
  * DMM_ERR_STATE on the two-kernel launch form. */
 dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double* out);
 
