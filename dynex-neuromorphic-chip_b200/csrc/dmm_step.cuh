@@ -553,10 +553,10 @@ __global__ void __launch_bounds__(kThreads) k_var(PackView<T> P, double* __restr
 
 // ---- persistent form -------------------------------------------------------------------------
 
-// Grid barrier for a cooperative launch: a monotonic arrival counter (zeroed before the
-// launch) and a bounded wait.  Returns false, after raising *err, when the wait gives up
-// (the co-residency of a cooperative launch makes this unreachable in practice; the bound
-// keeps a fault from turning into a hang).
+// Grid barrier for a cooperative launch: a monotonic arrival counter (zero at launch),
+// release-ordered arrivals, acquire-ordered polls and a bounded wait.  Returns false, after
+// raising *err, when the wait gives up (the co-residency of a cooperative launch makes this
+// unreachable in practice; the bound keeps a fault from turning into a hang).
 constexpr long long kBarrierSpinLimit = 1ll << 22;  // x ~0.3-1 us per poll: about a second
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
@@ -565,14 +565,24 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   return v;
 }
 
+// Arrival with release semantics: after the block barrier that precedes it, it makes the
+// whole block's earlier writes visible to a block that acquires the counter (release is
+// cumulative over what the thread has observed, and the block barrier orders the other
+// threads' writes before it).
+__device__ __forceinline__ void red_release(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_release64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 template <int NT>
 __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int& target, int* err,
                                              int* s_ok) {
   __syncthreads();
   target += gridDim.x;
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(bar, 1u);
+    red_release(bar, 1u);
     int ok = 1;
     long long it = 0;
     while (ld_acquire(bar) < target) {
@@ -583,8 +593,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int& ta
       }
       __nanosleep(64);
     }
-    __threadfence();
-    *s_ok = ok;
+    *s_ok = ok;  // the acquire load that saw the count orders everything after it
   }
   __syncthreads();
   return *s_ok != 0;

@@ -297,8 +297,7 @@ __global__ void __launch_bounds__(NT, 1)
     // ---- barrier 1 (split): phase B's own operands load during the wait
     __syncthreads();
     if (tid == 0) {
-      __threadfence();
-      atomicAdd(bar, 1u);
+      red_release(bar, 1u);
     }
     target += gridDim.x;
     uint32_t w[kXpPairs];
@@ -326,7 +325,6 @@ __global__ void __launch_bounds__(NT, 1)
         }
         __nanosleep(kPollSleepNs);
       }
-      __threadfence();
       s_ok = ok;
     }
     __syncthreads();
@@ -416,8 +414,7 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
         for (int i = 0; i < NT / 32; i++) km = max(km, cnt[0][i]);
       }
-      __threadfence();
-      atomicAdd(&acc->arrive, 1ull << (kArriveBits * km));
+      red_release64(&acc->arrive, 1ull << (kArriveBits * km));
       int ok = 1, kmax = 0;
       long long it = 0;
       for (;;) {
@@ -439,7 +436,6 @@ __global__ void __launch_bounds__(NT, 1)
         }
         __nanosleep(kPollSleepNs);
       }
-      __threadfence();
       s_ok = ok;
       trace_stamp(P, s, 8);
       const int loc = s_loc, vfail = s_vfail;
