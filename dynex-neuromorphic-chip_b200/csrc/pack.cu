@@ -485,8 +485,7 @@ static dmm_status upload_alpha(T* dst, const double* a, int32_t m, cudaStream_t 
 dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
                      const dmm_params* p, const double* alpha_cm, int32_t max_steps,
                      int32_t* idx_out) {
-  bool k3 = false, units = true;
-  DMM_TRY(validate_formula(lits, clause_off, n, m, &k3, &units));
+  DMM_TRY(validate_shape(lits, clause_off, n, m));
   if (alpha_cm && !with_alpha_cm_) {
     set_error("this pack was created without per-clause alpha storage");
     return DMM_ERR_ARG;
@@ -512,6 +511,18 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
     set_error("pack capacity exhausted (n=%d m=%d literals=%lld)", n, m, (long long)L);
     return DMM_ERR_BUDGET;
   }
+  // the literal upload runs while the host checks the clauses and literals
+  if (L > 0)
+    DMM_CUDA(cudaMemcpyAsync(lit_ + slot0, lits, (size_t)L * 4, cudaMemcpyHostToDevice, stream_));
+  bool k3 = false, units = true;
+  const dmm_status vst = validate_formula(lits, clause_off, n, m, &k3, &units);
+  if (vst != DMM_OK) {
+    cudaStreamSynchronize(stream_);
+    var_alloc_.free(var0, n);
+    cls_alloc_.free(cls0, m);
+    slot_alloc_.free(slot0, L);
+    return vst;
+  }
   InstDesc I{};
   I.n = n;
   I.m = m;
@@ -523,8 +534,6 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
   I.has_alpha_cm = alpha_cm ? 1 : 0;
   I.max_steps = max_steps;
   fill_params(I, p);
-  if (L > 0)
-    DMM_CUDA(cudaMemcpyAsync(lit_ + slot0, lits, (size_t)L * 4, cudaMemcpyHostToDevice, stream_));
   std::vector<int32_t> coff_local;
   if (!k3 && m > 0) {
     coff_local.resize(m);
