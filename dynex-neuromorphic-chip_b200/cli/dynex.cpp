@@ -3,19 +3,22 @@
 //
 //   dynex -i file.cnf [-l seed] [-w replicas] [-u walltime] [-z maxsteps]
 //         [-c alpha] [-b beta] [-n gamma] [-h delta] [-j epsilon] [-k zeta] [-m xl_max]
-//         [-q 0|1] [-P fp64|fp32] [-D device]
+//         [-q 0|1] [-p 0|1] [-P fp64|fp32] [-D device]
 //
 // Defaults follow the reference (FP64 arithmetic, seed 0, one replica); with them the
 // reported step count, T and assignment equal the reference's.  -P fp32 selects the
 // production FP32 path.  Replicas (-w) start from the reference's per-replica initial
 // states with alpha / i (dynex.cc:2643-2700) and run together in one batch; the replica
-// that solves at the lowest step wins.  Options of the reference that select modes
-// outside the default integrator (-o, -t, -p, -e, ...) are accepted and reported as
-// unsupported when they ask for anything but the default.
+// that solves at the lowest step wins.  -p 1 runs the reference's alpha heuristic every
+// 10^4 steps (one replica).  Options of the reference that select modes outside the
+// default integrator (-o, -t, -e, ...) are accepted and reported as unsupported when they
+// ask for anything but the default.
 #include <getopt.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -33,10 +36,57 @@ struct Opts {
   double walltime = 0.0;
   int max_steps = 0;
   bool quiet = false;
+  bool heuristics = false;
   dmm_precision prec = DMM_FP64;
   int device = 0;
   dmm_params p{};
 };
+
+constexpr int kHeuristicEvery = 10000;  // dynex.cc:1430
+
+struct HeuristicCounts {
+  int up = 0, down = 0, max = 0;
+  double median = 0.0;
+};
+
+// The reference's alpha heuristic (dynex.cc:1429-1457) on the state x after an accepted
+// step: clause alpha x1.1 where Xl is above the "median", x0.9 at or below it, floored at
+// the replica's alpha; a clause whose Xl reached xl_max gets the replica's alpha back and
+// Xl = alpha.  The median is the reference's own: nth_element around m/2, then the element
+// at index n, the variable count (dynex.cc:1108-1113).
+HeuristicCounts alpha_heuristic(std::vector<double>& x, std::vector<double>& acm, int n, int m,
+                                double alpha_replica, double alpha, double xl_max) {
+  HeuristicCounts h;
+  std::vector<double> v(x.begin() + n + m, x.begin() + n + 2 * (size_t)m);
+  const size_t nq = v.size() / 2;
+  std::nth_element(v.begin(), v.begin() + nq, v.end());
+  h.median = v[std::min<size_t>((size_t)n, v.size() - 1)];  // the reference reads v[n]
+  for (int i = 0; i < m; i++) {
+    const double xl = x[(size_t)n + m + i];
+    if (xl > h.median) {
+      acm[i] *= 1.1;
+      h.up++;
+    }
+    if (xl <= h.median) {
+      acm[i] *= 0.9;
+      h.down++;
+    }
+    if (acm[i] < alpha_replica) acm[i] = alpha_replica;
+    if (x[(size_t)n + m + i] >= xl_max) {
+      acm[i] = alpha_replica;
+      x[(size_t)n + m + i] = alpha;
+      h.max++;
+    }
+  }
+  return h;
+}
+
+// xl_max after the reference's `xl_max *= m` in int arithmetic (dynex.cc:2358)
+double effective_xl_max(int32_t factor, int32_t m) {
+  int32_t v = (int32_t)((uint32_t)factor * (uint32_t)m);
+  if (v <= 0) v = INT32_MAX;
+  return (double)v;
+}
 
 void usage(const char* argv0) {
   std::printf("c Syntax: %s -i file.cnf [options]\n", argv0);
@@ -94,9 +144,7 @@ int main(int argc, char** argv) {
       case 't':
         if (std::atoi(a) != 0) std::fprintf(stderr, "c -t %s: tuning mode is not available\n", a);
         break;
-      case 'p':
-        if (std::atoi(a) != 0) std::fprintf(stderr, "c -p %s: alpha heuristics are not available\n", a);
-        break;
+      case 'p': o.heuristics = std::atoi(a) != 0; break;
       default:
         break;  // other reference options only affect modes outside the default path
     }
@@ -124,6 +172,7 @@ int main(int argc, char** argv) {
     std::printf("c MAX VARIABLE OCCURENCE: %d\n", cnf->max_occurrence);
     std::printf("c PRECISION : %s\n", o.prec == DMM_FP64 ? "FP64" : "FP32");
     std::printf("c REPLICAS  : %d\n", o.replicas);
+    std::printf("c HEURISTICS: %d\n", o.heuristics ? 1 : 0);
     std::printf("c ALPHA %.15f BETA %.15f GAMMA %.15f DELTA %.15f EPSILON %.15f ZETA %.15f\n",
                 o.p.alpha, o.p.beta, o.p.gamma, o.p.delta, o.p.epsilon, o.p.zeta);
     std::printf("c SEED      : %d\n", o.seed);
@@ -149,8 +198,46 @@ int main(int argc, char** argv) {
       return EXIT_FAILURE;
     }
     if (!o.quiet) std::printf("c [0] STARTING ODE...\n");
-    dmm_limits lim{o.max_steps, 0, o.walltime};
-    if (fail(dmm_instance_solve(inst, &lim, &rep), "integration")) {
+    bool ok = true;
+    if (!o.heuristics) {
+      dmm_limits lim{o.max_steps, 0, o.walltime};
+      ok = !fail(dmm_instance_solve(inst, &lim, &rep), "integration");
+    } else {
+      // integrate to every 10^4-th step, apply the heuristic to the state there, continue
+      std::vector<double> acm((size_t)m, o.p.alpha);  // dmm_alpha_cm (dynex.cc:1201)
+      const double xl_max = effective_xl_max(o.p.xl_max, m);
+      ok = !fail(dmm_instance_set_params(inst, &o.p, acm.data()), "parameters");
+      while (ok) {
+        dmm_report cur{};
+        ok = !fail(dmm_instance_report(inst, &cur), "report");
+        int target = (cur.steps / kHeuristicEvery + 1) * kHeuristicEvery;
+        if (o.max_steps > 0) target = std::min(target, o.max_steps);
+        double wall = 0.0;
+        if (o.walltime > 0) {
+          wall = o.walltime - (now_s() - t0);
+          if (wall <= 0) break;
+        }
+        dmm_limits lim{target, 0, wall};
+        if (!ok || fail(dmm_instance_solve(inst, &lim, &rep), "integration")) {
+          ok = false;
+          break;
+        }
+        if (rep.status != DMM_STEP_LIMIT || rep.steps != target ||
+            (o.max_steps > 0 && rep.steps >= o.max_steps))
+          break;  // solved, out of time, or at the step cap
+        double t = 0.0;
+        if (fail(dmm_instance_get_state(inst, x.data(), &t), "state")) {
+          ok = false;
+          break;
+        }
+        const HeuristicCounts hc = alpha_heuristic(x, acm, n, m, o.p.alpha, o.p.alpha, xl_max);
+        std::printf("c [0] alpha heuristic changed %d up, %d down, %d max reached (median = %.2f)\n",
+                    hc.up, hc.down, hc.max, hc.median);
+        ok = !fail(dmm_instance_set_params(inst, &o.p, acm.data()), "parameters") &&
+             !fail(dmm_instance_set_state_at(inst, x.data(), t, rep.steps), "state");
+      }
+    }
+    if (!ok) {
       dmm_instance_destroy(inst);
       dmm_cnf_free(cnf);
       return EXIT_FAILURE;
@@ -166,6 +253,8 @@ int main(int argc, char** argv) {
   } else {
     dmm_batch* b = nullptr;
     const int R = o.replicas;
+    if (o.heuristics)
+      std::fprintf(stderr, "c -p: the alpha heuristic runs with one replica (-w 1) only\n");
     if (fail(dmm_batch_create(o.prec, o.device, R, (int64_t)n * R, (int64_t)m * R,
                               cnf->nlits * R, &b), "creating the batch")) {
       dmm_cnf_free(cnf);

@@ -151,6 +151,13 @@ dmm_status dmm_instance_set_state(dmm_instance* inst, const double* x) {
   return inst->pack->set_state(inst->idx, x);
 }
 
+dmm_status dmm_instance_set_state_at(dmm_instance* inst, const double* x, double t,
+                                     int32_t step) {
+  dmm::clear_error();
+  if (!inst || !x || step < 0) return DMM_ERR_ARG;
+  return inst->pack->set_state_at(inst->idx, x, t, step, true);
+}
+
 dmm_status dmm_instance_get_state(dmm_instance* inst, double* x, double* t) {
   dmm::clear_error();
   if (!inst) return DMM_ERR_ARG;

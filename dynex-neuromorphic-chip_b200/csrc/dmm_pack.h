@@ -88,6 +88,9 @@ class Pack {
   dmm_status set_max_steps(int32_t idx, int32_t max_steps);
   // State x (n+2m doubles) at t = 0, step 0; the instance becomes runnable.
   dmm_status set_state(int32_t idx, const double* x);
+  // The state x, the integration continuing at simulated time t after `step` accepted
+  // steps; keep_best keeps the best unsatisfied count seen so far.
+  dmm_status set_state_at(int32_t idx, const double* x, double t, int32_t step, bool keep_best);
   dmm_status get_state(int32_t idx, double* x, double* t);
   dmm_status rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, double* energy);
   dmm_status dostep(int32_t idx, const double* x, const double* dxdt, double h, double* xo);

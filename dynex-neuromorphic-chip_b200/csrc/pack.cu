@@ -625,7 +625,12 @@ dmm_status Pack::set_max_steps(int32_t idx, int32_t max_steps) {
 }
 
 dmm_status Pack::set_state(int32_t idx, const double* x) {
-  if (!live(idx) || !x) {
+  return set_state_at(idx, x, 0.0, 0, false);
+}
+
+dmm_status Pack::set_state_at(int32_t idx, const double* x, double t, int32_t step,
+                              bool keep_best) {
+  if (!live(idx) || !x || step < 0) {
     set_error("set_state: bad instance or null state");
     return DMM_ERR_ARG;
   }
@@ -647,8 +652,11 @@ dmm_status Pack::set_state(int32_t idx, const double* x) {
   DMM_CUDA(cudaGetLastError());
   InstCtrl c{};
   c.done = 0;
+  c.step = step;
+  c.t = t;
   c.loc = I.m;
-  c.best_loc = I.m;
+  c.best_loc = keep_best ? old.best_loc : I.m;
+  c.best_t = keep_best ? old.best_t : 0.0;
   c.solved_step = -1;
   c.solved_t = -1.0;
   c.h_state = 0.125;

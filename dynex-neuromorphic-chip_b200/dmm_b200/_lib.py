@@ -117,6 +117,7 @@ SIGNATURES = {
     "dmm_instance_set_tuning": (_i32, [_vp, _P(Tuning)]),
     "dmm_instance_get_tuning": (_i32, [_vp, _P(Tuning)]),
     "dmm_instance_set_state": (_i32, [_vp, _pd]),
+    "dmm_instance_set_state_at": (_i32, [_vp, _pd, _d, _i32]),
     "dmm_instance_get_state": (_i32, [_vp, _pd, _pd]),
     "dmm_instance_rhs": (_i32, [_vp, _pd, _pd, _pi32, _pd]),
     "dmm_instance_dostep": (_i32, [_vp, _pd, _pd, _d, _pd]),

@@ -100,6 +100,14 @@ class Instance:
             raise ValueError("state must have n + 2m entries")
         check(lib().dmm_instance_set_state(self._h, ptr(x, ctypes.c_double)))
 
+    def set_state_at(self, x, t: float, step: int) -> None:
+        """Sets the state with the integration continuing at time t after `step` steps."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.shape != (self.n + 2 * self.m,):
+            raise ValueError("state must have n + 2m entries")
+        check(lib().dmm_instance_set_state_at(self._h, ptr(x, ctypes.c_double), float(t),
+                                              int(step)))
+
     def get_state(self):
         x = np.zeros(self.n + 2 * self.m, dtype=np.float64)
         t = ctypes.c_double()

@@ -195,6 +195,13 @@ dmm_status dmm_instance_get_tuning(const dmm_instance* inst, dmm_tuning* t);
 /* Sets the state x (n + 2m doubles) at t = 0, step 0 (the initial_assignments of
  * dynex.cc:1216). */
 dmm_status dmm_instance_set_state(dmm_instance* inst, const double* x);
+/* Sets the state x with the integration continuing at simulated time t after `step`
+ * accepted steps, keeping the best unsatisfied count seen so far: the reference's
+ * continuation after its alpha heuristic rewrites Xl in the running state
+ * (dynex.cc:1429-1457), and its start from a loaded assignment at t_init
+ * (dynex.cc:2515-2540). */
+dmm_status dmm_instance_set_state_at(dmm_instance* inst, const double* x, double t,
+                                     int32_t step);
 /* Reads the current state (after the last accepted step) and simulated time. */
 dmm_status dmm_instance_get_state(dmm_instance* inst, double* x, double* t);
 /* Right-hand side of state x: replaces dmm_generate_dxdt (dynex.cc:332-720) without its

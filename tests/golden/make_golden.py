@@ -10,7 +10,14 @@ Outputs, next to this script:
                       and seed 0, 1, 2 (plus n = 10000, seed 0): printed step count, T,
                       and the reported `v` assignment; and the reference's per-step harness
                       (oracle/_ref/libdynex_ref.so) from a seeded uniform initial state:
-                      SHA-256 of the FP64 state at selected steps, solve step and T.
+                      SHA-256 of the FP64 state at selected steps, solve step and T;
+                      and the reference CLI with its alpha heuristic (-p 1) on a seeded
+                      planted formula (n = 2000, m = 8520, no clause agreeing with the
+                      planted assignment in all three literals) that needs more than 10^4
+                      steps: step count, T, the heuristic's printed counts and median, and
+                      the SHA-256 of the `v` assignment.
+
+    python tests/golden/make_golden.py --only heuristics   # adds/refreshes that entry only
 """
 from __future__ import annotations
 
@@ -45,13 +52,13 @@ def state_hash(x: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(x, dtype="<f8").tobytes()).hexdigest()
 
 
-def run_cli(path: str, seed: int, timeout: float = 600.0) -> dict:
+def run_cli(path: str, seed: int, timeout: float = 600.0, extra=()) -> dict:
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, os.path.basename(path))
         shutil.copy(path, p)
-        out = subprocess.run([REF_CLI, "-i", p, "-l", str(seed)], capture_output=True, text=True,
-                             timeout=timeout, cwd=d).stdout
-    text = out.replace("\r", "\n")
+        out = subprocess.run([REF_CLI, "-i", p, "-l", str(seed), *extra], capture_output=True,
+                             text=True, timeout=timeout, cwd=d).stdout
+    text = re.sub(r"\x1b\[[0-9;]*m", "", out.replace("\r", "\n"))
     # The progress line of the solving right-hand side carries T and the step counter
     # (dynex.cc:609-636); it is printed before the reference's display thread starts
     # writing, so it is never interleaved.
@@ -68,8 +75,32 @@ def run_cli(path: str, seed: int, timeout: float = 600.0) -> dict:
             v += [int(t) for t in line[2:].split()]
     if v and v[-1] == 0:
         v = v[:-1]
+    heur = [list(h.groups()) for h in re.finditer(
+        r"alpha heuristic changed (\d+) up, (\d+) down, (\d+) max reached \(median = ([0-9.]+)\)",
+        text)]
     return {"solved": m is not None, "T": float(m.group(1)) if m else None, "steps": steps,
-            "v": v}
+            "v": v, "heuristics": [[int(a), int(b), int(c), d] for a, b, c, d in heur]}
+
+
+HEURISTIC_FORMULA = {"n": 2000, "m": 8520, "p0": 0.0, "p1": 0.5, "seed": 16}
+
+
+def heuristics_case() -> dict:
+    """The reference CLI with -p 1 on HEURISTIC_FORMULA (made by this library's generator)."""
+    sys.path.insert(0, os.path.join(ROOT, "dynex-neuromorphic-chip_b200"))
+    import dmm_b200 as dmm
+    from dmm_b200.cnf import write_cnf
+    f = HEURISTIC_FORMULA
+    form, _ = dmm.generate_planted(f["n"], f["m"], f["p0"], f["p1"], seed=f["seed"])
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "heuristics.cnf")
+        write_cnf(form, path)
+        r = run_cli(path, 0, extra=("-p", "1"))
+    out = {"formula": f, "solved": r["solved"], "T": r["T"], "steps": r["steps"],
+           "heuristics": r["heuristics"],
+           "v_sha256": hashlib.sha256(np.array(r["v"], dtype="<i4").tobytes()).hexdigest()}
+    print("heuristics", out["steps"], out["T"], out["heuristics"], file=sys.stderr)
+    return out
 
 
 def planted_of(path: str):
@@ -84,8 +115,17 @@ def planted_of(path: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-dir", default="/root/reference")
+    ap.add_argument("--only", choices=["heuristics"], default=None)
     a = ap.parse_args()
     build()
+    if a.only == "heuristics":
+        path = os.path.join(HERE, "known_answers.json")
+        with open(path) as f:
+            answers = json.load(f)
+        answers["cli_heuristics"] = heuristics_case()
+        with open(path, "w") as f:
+            json.dump(answers, f, indent=1)
+        return
     paths = sorted(glob.glob(os.path.join(a.ref_dir, "cnf", "*.cnf")),
                    key=lambda p: int(re.search(r"_n_(\d+)_", p).group(1)))
     arrays = {}
@@ -119,6 +159,7 @@ def main():
             answers["cli"][f"{name}_seed0"]["v_sha256"] = hashlib.sha256(
                 np.array(r["v"], dtype="<i4").tobytes()).hexdigest()
             print(name, 0, r["steps"], r["T"], file=sys.stderr)
+    answers["cli_heuristics"] = heuristics_case()
     np.savez_compressed(os.path.join(HERE, "fixtures.npz"), **arrays)
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(answers, f, indent=1)

@@ -77,3 +77,26 @@ def test_cli_rejects_long_clause(tmp_path):
     r = subprocess.run([_lib.CLI_PATH, "-i", str(path)], capture_output=True, text=True)
     assert r.returncode != 0
     assert "MORE THAN 25 LITERALS" in r.stdout
+
+
+def test_cli_alpha_heuristic_matches_reference(tmp_path, known_answers):
+    """-p 1: the reference's alpha heuristic every 10^4 steps.  On a formula that needs more
+    than 10^4 steps, the printed heuristic counts and median, the step count, T and the
+    assignment equal the reference CLI's (the heuristic moves the solve from step 12164 to
+    13672 there)."""
+    import hashlib
+    ka = known_answers["cli_heuristics"]
+    f = ka["formula"]
+    form, _ = dmm.generate_planted(f["n"], f["m"], f["p0"], f["p1"], seed=f["seed"])
+    path = str(tmp_path / "heuristics.cnf")
+    dmm.write_cnf(form, path)
+    text = run_cli(["-i", path, "-p", "1"], timeout=600)
+    heur = [[int(a), int(b), int(c), d] for a, b, c, d in re.findall(
+        r"alpha heuristic changed (\d+) up, (\d+) down, (\d+) max reached \(median = ([0-9.]+)\)",
+        text)]
+    assert heur == ka["heuristics"]
+    out = parse(text)
+    assert out["sat"] and out["verified"]
+    assert out["steps"] == ka["steps"]
+    assert out["T"] == pytest.approx(ka["T"], abs=1e-9)
+    assert hashlib.sha256(np.array(out["v"], dtype="<i4").tobytes()).hexdigest() == ka["v_sha256"]
