@@ -193,7 +193,22 @@ class Pack {
   std::vector<int8_t> unit_h_;  // unit pins of the formula being added
   bool xp_active_ = false;
   bool one_active_ = false;
-  bool launch_area_clean_ = false;  // cooperative launch area zeroed (see leave_launch)  // single FP32 formula on the cooperative path
+  bool launch_area_clean_ = false;  // cooperative launch area zeroed (see leave_launch)
+  // which formula placement and tiling the staged tables were built for
+  struct XpKey {
+    int32_t idx;
+    int64_t var0, slot0;
+    int32_t n, m, tc, tv, g;
+    uint64_t serial;
+    bool operator==(const XpKey& o) const {
+      return idx == o.idx && var0 == o.var0 && slot0 == o.slot0 && n == o.n && m == o.m &&
+             tc == o.tc && tv == o.tv && g == o.g && serial == o.serial;
+    }
+  };
+  XpKey xp_key_{};
+  bool xp_key_valid_ = false;
+  std::vector<uint64_t> add_serial_;  // per slot: which add() placed the formula there
+  uint64_t add_counter_ = 0;  // single FP32 formula on the cooperative path
   enum { kXpDlist, kXpDoff, kXpLlit, kXpSpos, kXpUx, kXpUbase, kXpBoff, kXpSrc8, kXpDst,
          kXpScratch, kXpBufs };
   void* xbuf_[kXpBufs] = {};

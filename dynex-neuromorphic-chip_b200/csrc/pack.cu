@@ -270,6 +270,7 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   slot_alloc_.reset(S);
   inst_h_.assign(I, InstDesc{});
   live_.assign(I, 0);
+  add_serial_.assign(I, 0);
   tun_ = dmm_tuning{};
   DMM_TRY(set_tuning(&tun_));
   DMM_CUDA(cudaStreamSynchronize(stream_));
@@ -562,6 +563,7 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
   DMM_TRY(build_csr(I, lits));
   inst_h_[idx] = I;
   live_[idx] = 1;
+  add_serial_[idx] = ++add_counter_;
   DMM_TRY(upload_desc(idx));
   InstCtrl c{};
   c.done = DMM_CANCELLED;  // not runnable until a state is set
@@ -845,6 +847,14 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   *ok = false;
   const InstDesc& I = inst_h_[idx];
   if (prec_ != DMM_FP32 || !I.k3) return DMM_OK;
+  // the tables of the same formula at the same place with the same tiles are still valid
+  // (only this function writes them, and a live formula's device arrays do not change)
+  const XpKey key{idx, I.var0, I.slot0, I.n, I.m, TC, TV, tun_.var_group, add_serial_[idx]};
+  if (xp_key_valid_ && key == xp_key_) {
+    *ok = true;
+    return DMM_OK;
+  }
+  xp_key_valid_ = false;
   const int m = I.m, n = I.n, L = I.nslots;
   const int nct = (m + TC - 1) / TC, nvt = (n + TV - 1) / TV;
   if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_ || nvt > kXprepThreads)
@@ -926,6 +936,8 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   xbk_cap_ = bk_cap;
   xtv_cap_ = TV;
   xsmem_ = smem;
+  xp_key_ = key;
+  xp_key_valid_ = true;
   *ok = true;
   return DMM_OK;
 }
