@@ -99,6 +99,7 @@ dmm_status dmm_instance_create(const int32_t* lits, const int64_t* clause_off, i
   dmm::clear_error();
   if (!out || (precision != DMM_FP32 && precision != DMM_FP64)) return DMM_ERR_ARG;
   *out = nullptr;
+  dmm::DeviceScope device_scope(device);
   DMM_TRY(dmm::validate_shape(lits, clause_off, n, m));  // the rest is checked by add()
   auto* inst = new (std::nothrow) dmm_instance();
   if (!inst) return DMM_ERR_NOMEM;
@@ -125,7 +126,11 @@ dmm_status dmm_instance_create(const int32_t* lits, const int64_t* clause_off, i
   return DMM_OK;
 }
 
-void dmm_instance_destroy(dmm_instance* inst) { delete inst; }
+void dmm_instance_destroy(dmm_instance* inst) {
+  if (!inst) return;
+  dmm::DeviceScope device_scope(inst->pack ? inst->pack->device() : -1);
+  delete inst;
+}
 
 dmm_status dmm_instance_set_params(dmm_instance* inst, const dmm_params* p, const double* alpha_cm) {
   dmm::clear_error();
@@ -136,11 +141,13 @@ dmm_status dmm_instance_set_params(dmm_instance* inst, const dmm_params* p, cons
 dmm_status dmm_instance_set_tuning(dmm_instance* inst, const dmm_tuning* t) {
   dmm::clear_error();
   if (!inst || !t) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->set_tuning(t);
 }
 
 dmm_status dmm_instance_get_tuning(const dmm_instance* inst, dmm_tuning* t) {
   if (!inst || !t) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   *t = inst->pack->tuning();
   return DMM_OK;
 }
@@ -148,6 +155,7 @@ dmm_status dmm_instance_get_tuning(const dmm_instance* inst, dmm_tuning* t) {
 dmm_status dmm_instance_set_state(dmm_instance* inst, const double* x) {
   dmm::clear_error();
   if (!inst || !x) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->set_state(inst->idx, x);
 }
 
@@ -155,12 +163,14 @@ dmm_status dmm_instance_set_state_at(dmm_instance* inst, const double* x, double
                                      int32_t step) {
   dmm::clear_error();
   if (!inst || !x || step < 0) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->set_state_at(inst->idx, x, t, step, true);
 }
 
 dmm_status dmm_instance_get_state(dmm_instance* inst, double* x, double* t) {
   dmm::clear_error();
   if (!inst) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->get_state(inst->idx, x, t);
 }
 
@@ -168,6 +178,7 @@ dmm_status dmm_instance_rhs(dmm_instance* inst, const double* x, double* dxdt, i
                             double* energy) {
   dmm::clear_error();
   if (!inst || !x || !dxdt) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->rhs(inst->idx, x, dxdt, loc, energy);
 }
 
@@ -175,12 +186,14 @@ dmm_status dmm_instance_dostep(dmm_instance* inst, const double* x, const double
                                double* x_out) {
   dmm::clear_error();
   if (!inst || !x || !dxdt || !x_out) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->dostep(inst->idx, x, dxdt, h, x_out);
 }
 
 dmm_status dmm_instance_report(dmm_instance* inst, dmm_report* rep) {
   dmm::clear_error();
   if (!inst || !rep) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   InstCtrl c;
   DMM_TRY(inst->pack->read_ctrl(inst->idx, &c));
   fill_report(c, rep);
@@ -191,6 +204,7 @@ dmm_status dmm_instance_report(dmm_instance* inst, dmm_report* rep) {
 dmm_status dmm_instance_step(dmm_instance* inst, int32_t nsteps, dmm_report* rep) {
   dmm::clear_error();
   if (!inst || nsteps < 0) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   const double t0 = now_s();
   InstCtrl c;
   DMM_TRY(inst->pack->read_ctrl(inst->idx, &c));
@@ -212,6 +226,7 @@ dmm_status dmm_instance_step(dmm_instance* inst, int32_t nsteps, dmm_report* rep
 dmm_status dmm_instance_solve(dmm_instance* inst, const dmm_limits* lim, dmm_report* rep) {
   dmm::clear_error();
   if (!inst) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   const double t0 = now_s();
   const int32_t max_steps = lim && lim->max_steps > 0 ? lim->max_steps : 0;
   const double wall = lim ? lim->wall_s : 0.0;
@@ -228,6 +243,7 @@ dmm_status dmm_instance_solve(dmm_instance* inst, const dmm_limits* lim, dmm_rep
 dmm_status dmm_instance_assignment(dmm_instance* inst, int8_t* pre, int8_t* post) {
   dmm::clear_error();
   if (!inst) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->assignment(inst->idx, pre, post);
 }
 
@@ -235,6 +251,7 @@ dmm_status dmm_instance_profile(dmm_instance* inst, int32_t nsteps, int64_t flus
                                 double* clause_ms, double* var_ms) {
   dmm::clear_error();
   if (!inst || nsteps < 0 || flush_bytes < 0) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   dmm::StepTimes t;
   DMM_TRY(inst->pack->profile_steps(nsteps, flush_bytes, &t));
   if (clause_ms) *clause_ms = t.clause_ms;
@@ -245,6 +262,7 @@ dmm_status dmm_instance_profile(dmm_instance* inst, int32_t nsteps, int64_t flus
 dmm_status dmm_instance_time_steps(dmm_instance* inst, int32_t nsteps, double* ms) {
   dmm::clear_error();
   if (!inst || nsteps < 0 || !ms) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   cudaEvent_t e0, e1;
   DMM_CUDA(cudaEventCreate(&e0));
   DMM_CUDA(cudaEventCreate(&e1));
@@ -264,17 +282,20 @@ dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
                                            int64_t flush_bytes, double* ms) {
   dmm::clear_error();
   if (!inst || nsteps < 0 || flush_bytes < 0 || !ms) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->time_steps_flushed(nsteps, flush_bytes, ms);
 }
 
 int32_t dmm_instance_launch_form(const dmm_instance* inst) {
   if (!inst) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->launch_form();
 }
 
 dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double* out) {
   dmm::clear_error();
   if (!inst || nsteps <= 0 || !out) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
   return inst->pack->trace_phases(nsteps, out);
 }
 
@@ -288,6 +309,7 @@ dmm_status dmm_batch_create(dmm_precision precision, int32_t device, int32_t max
       (precision != DMM_FP32 && precision != DMM_FP64))
     return DMM_ERR_ARG;
   *out = nullptr;
+  dmm::DeviceScope device_scope(device);
   auto* b = new (std::nothrow) dmm_batch();
   if (!b) return DMM_ERR_NOMEM;
   b->pack.reset(new (std::nothrow) Pack(precision, device));
@@ -305,7 +327,11 @@ dmm_status dmm_batch_create(dmm_precision precision, int32_t device, int32_t max
   return DMM_OK;
 }
 
-void dmm_batch_destroy(dmm_batch* b) { delete b; }
+void dmm_batch_destroy(dmm_batch* b) {
+  if (!b) return;
+  dmm::DeviceScope device_scope(b->pack ? b->pack->device() : -1);
+  delete b;
+}
 
 dmm_status dmm_batch_set_tuning(dmm_batch* b, const dmm_tuning* t) {
   dmm::clear_error();
@@ -319,6 +345,7 @@ dmm_status dmm_batch_add(dmm_batch* b, const int32_t* lits, const int64_t* claus
                          int32_t* index) {
   dmm::clear_error();
   if (!b || !x0 || !index) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(b->pack->device());
   int32_t idx = -1;
   DMM_TRY(b->pack->add(lits, clause_off, n, m, p, nullptr, max_steps, &idx));
   dmm_status st = b->pack->set_state(idx, x0);
@@ -341,6 +368,7 @@ dmm_status dmm_batch_run_until(dmm_batch* b, double wall_s, int32_t stop_after,
                                dmm_batch_stats* stats) {
   dmm::clear_error();
   if (!b || stop_after < 0) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(b->pack->device());
   if (b->dirty) {
     DMM_TRY(b->pack->commit_tiles());
     b->dirty = false;
@@ -389,6 +417,7 @@ dmm_status dmm_batch_run_until(dmm_batch* b, double wall_s, int32_t stop_after,
 dmm_status dmm_batch_result(dmm_batch* b, int32_t index, dmm_report* rep, int8_t* post) {
   dmm::clear_error();
   if (!b || index < 0 || index >= (int32_t)b->idx.size()) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(b->pack->device());
   const int32_t i = b->idx[index];
   if (rep) {
     InstCtrl c;
@@ -402,12 +431,14 @@ dmm_status dmm_batch_result(dmm_batch* b, int32_t index, dmm_report* rep, int8_t
 dmm_status dmm_batch_assignment(dmm_batch* b, int32_t index, int8_t* pre, int8_t* post) {
   dmm::clear_error();
   if (!b || index < 0 || index >= (int32_t)b->idx.size()) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(b->pack->device());
   return b->pack->assignment(b->idx[index], pre, post);
 }
 
 dmm_status dmm_batch_state(dmm_batch* b, int32_t index, double* x, double* t) {
   dmm::clear_error();
   if (!b || index < 0 || index >= (int32_t)b->idx.size()) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(b->pack->device());
   return b->pack->get_state(b->idx[index], x, t);
 }
 

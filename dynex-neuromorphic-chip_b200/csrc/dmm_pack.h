@@ -36,6 +36,23 @@ const char* last_error();
     if (s_ != DMM_OK) return s_;          \
   } while (0)
 
+// Makes `dev` the calling thread's current device for the scope of a library call and
+// restores the caller's device afterwards (every entry point that takes a handle).
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    if (dev >= 0 && dev != prev) cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 // Validates a formula given as flat literals + offsets.  Sets *k3 when every clause has
 // exactly three literals, and *may_have_units (if given) unless every clause has two or more.
 dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n,

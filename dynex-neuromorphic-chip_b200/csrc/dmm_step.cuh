@@ -695,7 +695,10 @@ __global__ void __launch_bounds__(NT, 1)
       clause_tile<T, VEC, NT>(P, sm, ti);
     }
     stamp(s, 3);
-    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    if (!grid_barrier<NT>(bar, target, err, &s_ok)) {
+      leave_launch(bar);  // every block gives up in turn; the last one clears the area
+      return;
+    }
     stamp(s, 4);
     if (ONE && blockIdx.x == 0 && threadIdx.x == 0) {
       StepAcc* z = P.acc2 + ((s + 1) & 1);
@@ -713,7 +716,10 @@ __global__ void __launch_bounds__(NT, 1)
       var_tile<T, G, SORTED, 0, NT>(P, sm, nullptr);
     }
     stamp(s, 7);
-    if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+    if (!grid_barrier<NT>(bar, target, err, &s_ok)) {
+      leave_launch(bar);  // every block gives up in turn; the last one clears the area
+      return;
+    }
     stamp(s, 8);
     if constexpr (ONE) {
       if (threadIdx.x == 0) {
@@ -747,7 +753,10 @@ __global__ void __launch_bounds__(NT, 1)
         __syncthreads();
       }
       stamp(s, 9);
-      if (!grid_barrier<NT>(bar, target, err, &s_ok)) return;
+      if (!grid_barrier<NT>(bar, target, err, &s_ok)) {
+      leave_launch(bar);  // every block gives up in turn; the last one clears the area
+      return;
+    }
     }
   }
   leave_launch(bar);

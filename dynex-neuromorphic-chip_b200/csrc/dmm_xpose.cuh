@@ -328,7 +328,10 @@ __global__ void __launch_bounds__(NT, 1)
       s_ok = ok;
     }
     __syncthreads();
-    if (!s_ok) return;
+    if (!s_ok) {
+      leave_launch(bar);  // every block gives up in turn; the last one clears the area
+      return;
+    }
     trace_stamp(P, s, 4);
 
     // the step's counts of phase A, used by the decision after barrier 2
@@ -480,7 +483,10 @@ __global__ void __launch_bounds__(NT, 1)
       lc.pending = 1;
     }
     __syncthreads();
-    if (!s_ok) return;
+    if (!s_ok) {
+      leave_launch(bar);  // every block gives up in turn; the last one clears the area
+      return;
+    }
     trace_stamp(P, s, 9);
   }
   leave_launch(bar);

@@ -1086,12 +1086,9 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
 template <int G>
 static dmm_status launch_inst_g(const PackView<float>& v, const int32_t* order, int count,
                                 int nsteps, int* queue, int grid, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    DMM_CUDA(cudaFuncSetAttribute(k_inst<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kInstSmem));
-    attr = true;
-  }
+  // function attributes are per device: set it on the current one (a cheap driver call)
+  DMM_CUDA(cudaFuncSetAttribute(k_inst<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kInstSmem));
   k_inst<G><<<grid, kInstThreads, kInstSmem, s>>>(v, order, count, nsteps, queue);
   DMM_CUDA(cudaGetLastError());
   return DMM_OK;

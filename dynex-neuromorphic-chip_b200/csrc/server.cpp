@@ -63,6 +63,7 @@ dmm_status dmm_server_create(const dmm_server_config* cfg, dmm_server** out) {
       (cfg->precision != DMM_FP32 && cfg->precision != DMM_FP64))
     return DMM_ERR_ARG;
   *out = nullptr;
+  dmm::DeviceScope device_scope(cfg->device);
   auto* s = new (std::nothrow) dmm_server();
   if (!s) return DMM_ERR_NOMEM;
   s->cfg = *cfg;
@@ -96,7 +97,11 @@ dmm_status dmm_server_create(const dmm_server_config* cfg, dmm_server** out) {
   return DMM_OK;
 }
 
-void dmm_server_destroy(dmm_server* s) { delete s; }
+void dmm_server_destroy(dmm_server* s) {
+  if (!s) return;
+  dmm::DeviceScope device_scope(s->pack ? s->pack->device() : -1);
+  delete s;
+}
 
 double dmm_server_clock(dmm_server* s) { return s ? s->clock() : 0.0; }
 
@@ -206,6 +211,7 @@ static dmm_status admit(dmm_server* s, bool* changed) {
 dmm_status dmm_server_pump(dmm_server* s, int32_t* resident, int32_t* queued) {
   dmm::clear_error();
   if (!s) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(s->pack->device());
   DMM_TRY(retire(s));
   bool changed = false;
   DMM_TRY(admit(s, &changed));
@@ -228,6 +234,7 @@ dmm_status dmm_server_pump(dmm_server* s, int32_t* resident, int32_t* queued) {
 dmm_status dmm_server_take(dmm_server* s, dmm_server_result* out, int32_t cap, int32_t* count) {
   dmm::clear_error();
   if (!s || !count || cap < 0 || (cap > 0 && !out)) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(s->pack->device());
   const int32_t k = std::min<int32_t>(cap, (int32_t)s->finished.size());
   for (int32_t i = 0; i < k; i++) out[i] = s->finished[i];
   s->finished.erase(s->finished.begin(), s->finished.begin() + k);
@@ -238,6 +245,7 @@ dmm_status dmm_server_take(dmm_server* s, dmm_server_result* out, int32_t cap, i
 dmm_status dmm_server_assignment(dmm_server* s, int64_t ticket, int8_t* post, int32_t n) {
   dmm::clear_error();
   if (!s || !post) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(s->pack->device());
   auto it = s->assignments.find(ticket);
   if (it == s->assignments.end()) {
     dmm::set_error("no finished assignment for ticket %lld", (long long)ticket);
