@@ -286,6 +286,13 @@ dmm_status dmm_instance_time_steps_flushed(dmm_instance* inst, int32_t nsteps,
   return inst->pack->time_steps_flushed(nsteps, flush_bytes, ms);
 }
 
+dmm_status dmm_instance_test_barrier_timeout(dmm_instance* inst) {
+  dmm::clear_error();
+  if (!inst) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(inst->pack->device());
+  return inst->pack->test_barrier_timeout();
+}
+
 int32_t dmm_instance_launch_form(const dmm_instance* inst) {
   if (!inst) return DMM_ERR_ARG;
   dmm::DeviceScope device_scope(inst->pack->device());

@@ -125,6 +125,9 @@ struct PackView {
   // clock counts
   long long* trace;
   int32_t trace_steps;
+  // test hook: arrivals the first grid barrier of a launch waits for beyond the grid (0
+  // normally; 1 makes every block's bounded wait run out)
+  int32_t barrier_extra;
 };
 
 // ---- exactly rounded arithmetic (no FMA contraction: the reference has none) ----------

@@ -137,6 +137,9 @@ class Pack {
   // Kernel used by launch_steps: 1 two-kernel, 2 cooperative, 3 cooperative single formula,
   // 4 staged, 5 one block per formula (dmm_instance_launch_form).
   int launch_form() const;
+  // Test hook: one cooperative launch whose first grid barrier waits for one arrival more
+  // than the grid has; returns what check_error reports (DMM_ERR_CUDA).
+  dmm_status test_barrier_timeout();
   // Loads every kernel this pack's precision and tuning can launch (the driver otherwise
   // loads a kernel at its first launch, which would stall a running service).
   dmm_status preload_kernels();
@@ -211,6 +214,7 @@ class Pack {
   bool xp_active_ = false;
   bool one_active_ = false;
   bool launch_area_clean_ = false;  // cooperative launch area zeroed (see leave_launch)
+  int32_t barrier_extra_ = 0;       // test_barrier_timeout
   // which formula placement and tiling the staged tables were built for
   struct XpKey {
     int32_t idx;

@@ -695,6 +695,7 @@ __global__ void __launch_bounds__(NT, 1)
       clause_tile<T, VEC, NT>(P, sm, ti);
     }
     stamp(s, 3);
+    if (s == 0) target += P.barrier_extra;
     if (!grid_barrier<NT>(bar, target, err, &s_ok)) {
       leave_launch(bar);  // every block gives up in turn; the last one clears the area
       return;

@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(NT, 1)
     if (tid == 0) {
       red_release(bar, 1u);
     }
-    target += gridDim.x;
+    target += gridDim.x + (s == 0 ? P.barrier_extra : 0);
     uint32_t w[kXpPairs];
     T cv = T(0);
     const int nv = has_v ? vtile.count : 0, v0 = has_v ? vtile.begin : 0;

@@ -736,6 +736,7 @@ void Pack::fill_view(void* vv) const {
   v.xsv_cap = xsv_cap_;
   v.xbk_cap = xbk_cap_;
   v.xtv_cap = xtv_cap_;
+  v.barrier_extra = barrier_extra_;
   v.trace = trace_on_ ? trace_ : nullptr;
   v.trace_steps = trace_on_ ? trace_steps_ : 0;
 }
@@ -1119,10 +1120,26 @@ dmm_status Pack::check_error() {
   DMM_CUDA(cudaStreamSynchronize(stream_));
   if (e) {
     launch_area_clean_ = false;
+    DMM_CUDA(cudaMemsetAsync(misc_d_ + 1, 0, sizeof(int32_t), stream_));  // reported once
+    DMM_CUDA(cudaStreamSynchronize(stream_));
     set_error("grid barrier wait gave up in the cooperative step kernel");
     return DMM_ERR_CUDA;
   }
   return DMM_OK;
+}
+
+dmm_status Pack::test_barrier_timeout() {
+  DMM_CUDA(cudaSetDevice(dev_));
+  if (tun_.launch_mode == 1 || (ctiles_h_.empty() && vtiles_h_.empty())) {
+    set_error("the barrier test needs the cooperative launch of tile-path formulas");
+    return DMM_ERR_STATE;
+  }
+  barrier_extra_ = 1;
+  const dmm_status st = launch_persist(1);
+  barrier_extra_ = 0;
+  DMM_TRY(st);
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  return check_error();
 }
 
 dmm_status Pack::capture(int32_t steps) {

@@ -130,6 +130,7 @@ SIGNATURES = {
     "dmm_instance_time_steps_flushed": (_i32, [_vp, _i32, _i64, _pd]),
     "dmm_instance_trace_phases": (_i32, [_vp, _i32, _pd]),
     "dmm_instance_launch_form": (_i32, [_vp]),
+    "dmm_instance_test_barrier_timeout": (_i32, [_vp]),
     "dmm_rhs3_f32_noalloc": (_i32, [_vp, _i32, _i32, _vp, _P(Params), _vp, _vp, _vp]),
     "dmm_batch_create": (_i32, [_i32, _i32, _i32, _i64, _i64, _i64, _P(_vp)]),
     "dmm_batch_destroy": (None, [_vp]),

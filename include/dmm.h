@@ -233,6 +233,12 @@ dmm_status dmm_instance_assignment(dmm_instance* inst, int8_t* pre, int8_t* post
  *   5  one block per formula
  * or a negative dmm_status. */
 int32_t dmm_instance_launch_form(const dmm_instance* inst);
+/* No counterpart in the reference.  Test hook for the failure path of the cooperative step
+ * kernels: one launch whose first grid barrier waits for one arrival more than the grid has,
+ * so every block's bounded wait runs out (a few seconds); returns the status the library
+ * reports for it (DMM_ERR_CUDA, "grid barrier wait gave up ...").  The device context stays
+ * usable; the instance's state is undefined afterwards (set a state before stepping). */
+dmm_status dmm_instance_test_barrier_timeout(dmm_instance* inst);
 /* Benchmark helper: runs nsteps steps as plain launches with CUDA events around each of
  * the two step kernels; before each step it writes flush_bytes of scratch (0: none) so
  * the step starts with a cold L2.  Returns the summed device times (ms). */
