@@ -252,6 +252,57 @@ def run_reference_arm(a):
 
 # ---- our arm ------------------------------------------------------------------------------
 
+class Ranks:
+    """One process per GPU (torchrun): barrier, max / sum / any over ranks.  The run shards
+    nothing (each rank integrates its own replica), so these are the only collectives, and
+    every rank takes them in the same order.  backend "nccl" with device "cuda:<local>" on
+    GPUs; "gloo" with device "cpu" in the multi-process CPU tests."""
+
+    def __init__(self, world: int, backend: str = "nccl", device: str = "cpu"):
+        import torch
+
+        self.torch = torch
+        self.world = world
+        self.device = device
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.device.startswith("cuda"):
+            self.torch.cuda.synchronize()
+
+    def _reduce(self, x: float, op) -> float:
+        if self.dist is None:
+            return float(x)
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.MAX if self.dist else None)
+
+    def sum(self, x: float) -> float:
+        return self._reduce(x, self.dist.ReduceOp.SUM if self.dist else None)
+
+    def any(self, flag: bool) -> bool:
+        """True on every rank when the flag is set on any rank (collective decisions)."""
+        return self.max(1.0 if flag else 0.0) > 0.0
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -272,33 +323,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
     if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks(world, "nccl", f"cuda:{local}")
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     form, x0 = make_instance(rank)
     n, m = form.n, form.m
@@ -315,9 +343,10 @@ def main():
             step_ms = inst.time_steps_flushed(K, FLUSH_BYTES)
         barrier()
         steps_done = inst.report().steps - s0
-        if steps_done == K:
+        # a replica that solved inside the timed region did no-op steps: every rank restarts
+        # (the decision is collective, so all ranks take the same barriers)
+        if not ranks.any(steps_done != K):
             break
-        # solved inside the timed region: the remaining steps would be no-ops; restart
         init_seed += 1000
         x0 = dmm.initial_state_uniform(form, init_seed)
     clocks = clk.summary()
@@ -411,9 +440,7 @@ def main():
             line.update(extras)
         print(json.dumps(line), flush=True)
     inst.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
