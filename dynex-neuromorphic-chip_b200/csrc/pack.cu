@@ -163,6 +163,12 @@ inline int blocks_for(int64_t work, int per = kThreads, int cap = 148 * 16) {
 constexpr int kMinClauseTile = 256;  // smallest clause tile (bounds the tile tables)
 constexpr int kMinVarTile = 32;      // smallest variable tile
 constexpr int kPersistThreads = 1024;  // block size of the cooperative step kernel
+// FP64: 512 threads, so that the sorted sums and the clause code fit in registers without
+// spilling (measured 74.3 vs 76.4 us per n=100k step with 1024 threads)
+constexpr int kPersistThreads64 = 512;
+static int persist_threads(dmm_precision prec) {
+  return prec == DMM_FP64 ? kPersistThreads64 : kPersistThreads;
+}
 constexpr int kXpSmemMax = 220 * 1024;  // dynamic shared memory of the staged form, at most
 constexpr int kMiscInts = 48;            // misc_d_: 192 bytes
 constexpr int kMiscLaunch = 16;          // misc_d_ index of the per-launch area (byte 64)
@@ -811,7 +817,7 @@ static int occupancy_blocks(const void* fn, int threads, size_t smem = 0) {
 // ONE: single-formula form (FP32 only)
 template <bool ONE>
 static const void* persist_fn_x(dmm_precision prec, int G) {
-  if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads>;
+  if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads64>;
   switch (G) {
     case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, ONE>;
     case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, ONE>;
@@ -992,9 +998,9 @@ dmm_status Pack::commit_tiles() {
     bc = std::min(bc, tun_.blocks_per_sm);
     bv = std::min(bv, tun_.blocks_per_sm);
   }
-  grid_p_ = occupancy_blocks(persist_fn(), kPersistThreads) * sms_;
+  grid_p_ = occupancy_blocks(persist_fn(), persist_threads(prec_)) * sms_;
   const bool coop = tun_.launch_mode != 1;
-  const int block = coop ? kPersistThreads : kThreads;
+  const int block = coop ? persist_threads(prec_) : kThreads;
   const int64_t spread = coop ? grid_p_ : (int64_t)bc * sms_;
   // tile sizes: balanced over the grid for a single instance, else fixed
   int TC = tun_.clause_tile, TV = tun_.var_tile;
@@ -1079,7 +1085,7 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
   const size_t smem = xp_active_ ? (size_t)xsmem_ : 0;
   if (smem)
     DMM_CUDA(cudaFuncSetAttribute(persist_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(kPersistThreads), args,
+  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(persist_threads(prec_)), args,
                                        smem, stream_));
   return DMM_OK;
 }
