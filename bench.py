@@ -58,7 +58,10 @@ def parse():
     ap.add_argument("--precision-study", action="store_true",
                     help="only run the FP32-vs-FP64 study (n=1,000,000) and print its line")
     ap.add_argument("--study-n", type=int, default=1_000_000)
-    ap.add_argument("--study-seeds", type=int, default=16)
+    ap.add_argument("--study-seeds", type=int, default=64)
+    ap.add_argument("--study-ratio", type=float, default=8.0,
+                    help="clause-to-variable ratio of the study's formula")
+    ap.add_argument("--study-max-steps", type=int, default=5000)
     return ap.parse_args()
 
 
@@ -70,8 +73,11 @@ def run_extras(device: int) -> dict:
 
     from dmm_b200 import workloads as w
 
+    from dmm_b200.tuner import autotune_batch
+
     items = w.make_items(4096, 100, 5000, ratios=(8.0,), seed=1)
-    b = w.run_batched(items, max_steps=2000, device=device)
+    tuned = autotune_batch(items, max_steps=2000, device=device)
+    b = w.run_batched(items, max_steps=2000, tuning=tuned["best"], device=device)
     sample = items[:64]
     p = w.run_plain(sample, max_steps=2000, device=device)
     pb = w.run_batched(sample, max_steps=2000, device=device)
@@ -89,6 +95,10 @@ def run_extras(device: int) -> dict:
                          "clause_updates_per_s": p["clause_updates_per_s"],
                          "path": "dmm_instance create + solve, one formula at a time"},
         "batched_same_sample_solves_per_s": pb["solves_per_s_run"],
+        "autotune": {"best": tuned["best"],
+                     "sample_device_ms": {f"var_group={g},steps_per_graph={sp}": round(ms, 3)
+                                          for (g, sp), ms in tuned["table"]},
+                     "note": "first 512 formulas, each shape; results identical for every shape"},
         "solves_ratio_vs_plain": b["solves_per_s_run"] / max(p["solves_per_s"], 1e-9),
     }
     sv = w.make_items(300, 100, 100000, ratios=(4.3, 6.0, 8.0), seed=2)
@@ -311,9 +321,11 @@ def main():
     if a.precision_study:
         from dmm_b200 import workloads as w
 
-        r = w.precision_study(n=a.study_n, seeds=range(a.study_seeds))
+        r = w.precision_study(n=a.study_n, r=a.study_ratio, seeds=range(a.study_seeds),
+                              max_steps=a.study_max_steps)
         print(json.dumps({"precision_study": r, "workload": f"planted 3-SAT n={a.study_n}, "
-                          "r=8, p0=0.08, FP32 vs FP64 from the same initial states"}), flush=True)
+                          f"r={a.study_ratio:g}, p0=0.08, FP32 vs FP64 from the same initial "
+                          "states"}), flush=True)
         return
     import numpy as np
     import torch

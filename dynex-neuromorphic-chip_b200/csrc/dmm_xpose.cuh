@@ -16,7 +16,7 @@
 //      in shared memory, then reduces each variable from there.
 //
 // Grid barriers are split (arrive ... wait) so that loads that do not depend on the other
-// blocks (the destination positions and voltages of phase B) are in flight during the wait.
+// blocks (the voltages of phase B's variables) are in flight during the wait.
 // Barrier 2 carries the step decision: a block arrives by adding 1 << (12 k) to the step's
 // arrival word, k = the largest trial index of its variables, so that the word that ends
 // the wait also holds the step's largest trial index.  The step's unsatisfied count and
@@ -30,7 +30,6 @@
 namespace dmm {
 
 constexpr uint16_t kXpPad = 0xFFFF;  // xdst of a padding entry
-constexpr int kXpPairs = 10;         // destination pairs per thread loaded across barrier 1
 constexpr int kArriveBits = 12;      // width of one trial's arrival count (> grid size)
 constexpr int kPollSleepNs = 64;     // back-off between polls of a barrier word
 
@@ -294,24 +293,18 @@ __global__ void __launch_bounds__(NT, 1)
     }
     trace_stamp(P, s, 3);
 
-    // ---- barrier 1 (split): phase B's own operands load during the wait
+    // ---- barrier 1 (split): the variable tile's voltages load during the wait
     __syncthreads();
     if (tid == 0) {
       red_release(bar, 1u);
     }
     target += gridDim.x + (s == 0 ? P.barrier_extra : 0);
-    uint32_t w[kXpPairs];
     T cv = T(0);
     const int nv = has_v ? vtile.count : 0, v0 = has_v ? vtile.begin : 0;
     const uint32_t* __restrict__ xd2 =
         reinterpret_cast<const uint32_t*>(P.xdst + bbeg);  // positions, two per word
     const int nb2 = blen / 2;
     if (has_v) {
-#pragma unroll
-      for (int k = 0; k < kXpPairs; k++) {
-        const int q = tid + k * NT;
-        w[k] = q < nb2 ? __ldg(xd2 + q) : 0xFFFFFFFFu;
-      }
       if (tid < nv) cv = V[v0 + tid];  // V(step) of the tile's variables
     }
     if (tid == 0) {
@@ -362,12 +355,7 @@ __global__ void __launch_bounds__(NT, 1)
           if (pos != kXpPad) cp_async4(bucket + pos, P.ux + s_src8[p >> 3] + (p & 7));
         }
       };
-#pragma unroll
-      for (int k = 0; k < kXpPairs; k++) {
-        const int q = tid + k * NT;
-        if (q < nb2) issue(q, w[k]);
-      }
-      for (int q = tid + kXpPairs * NT; q < nb2; q += NT) issue(q, __ldg(xd2 + q));
+      for (int q = tid; q < nb2; q += NT) issue(q, __ldg(xd2 + q));
       if (tid < nv) s_cur[tid] = cv;
       for (int i = tid + NT; i < nv; i += NT) s_cur[i] = V[v0 + i];
       cp_async_wait_all();

@@ -50,3 +50,27 @@ def autotune(inst: Instance, x0, steps: int = 6, flush_bytes: int = 0, var_group
     inst.set_tuning(**best)
     inst.set_state(x0)
     return {"best": best, "table": table, "graph_table": gtable}
+
+
+BATCH_VAR_GROUPS = (1, 4, 8, 32)
+BATCH_STEPS_PER_GRAPH = (16, 64, 256)
+
+
+def autotune_batch(items, max_steps: int, var_groups=BATCH_VAR_GROUPS,
+                   steps_per_graph=BATCH_STEPS_PER_GRAPH, sample: int = 512,
+                   device: int = 0) -> dict:
+    """Batched configuration: integrates the same sample of formulas (the first `sample`
+    items, each from its own initial state, to the step cap or its solution) under every
+    (lanes per variable, steps per CUDA graph) shape and keeps the shape with the lowest
+    device time.  Results are identical for every shape, so only time decides.  Returns
+    {"best": {"var_group": g, "steps_per_graph": s}, "table": [((g, s), device_ms), ...]}."""
+    from .workloads import run_batched
+
+    part = items[:sample]
+    table = []
+    for g, s in itertools.product(var_groups, steps_per_graph):
+        r = run_batched(part, max_steps, tuning=dict(var_group=g, steps_per_graph=s),
+                        device=device)
+        table.append(((g, s), r["device_ms"]))
+    (g, s), _ = min(table, key=lambda r: r[1])
+    return {"best": {"var_group": g, "steps_per_graph": s}, "table": table}

@@ -99,9 +99,12 @@ def precision_study(n: int = 1_000_000, r: float = 8.0, seeds=range(8),
                     device: int = 0) -> dict:
     """FP32 production path against the FP64 path (the reference's arithmetic) on one planted
     formula from several initial states: max |dV| and |dXl| at each checkpoint step (while
-    both runs are still integrating), then solve rate and steps-to-solution of each."""
+    both runs are still integrating), then solve rate and steps-to-solution of each.  A run
+    in which either precision stopped (solved) before a checkpoint is counted under that
+    checkpoint's "stopped_before" instead."""
     f, _ = generate_planted(n, int(round(r * n)), 0.08, 0.46, seed=instance_seed)
     errs = {c: {"dv": [], "dxl": []} for c in checkpoints}
+    stopped = {c: 0 for c in checkpoints}
     res = {"fp32": [], "fp64": []}
     i32 = Instance(f, precision="fp32", device=device)
     i64 = Instance(f, precision="fp64", device=device)
@@ -111,11 +114,13 @@ def precision_study(n: int = 1_000_000, r: float = 8.0, seeds=range(8),
             i32.set_state(x0)
             i64.set_state(x0)
             done = 0
-            for c in checkpoints:
+            for k, c in enumerate(checkpoints):
                 a = i32.step(c - done)
                 b = i64.step(c - done)
                 done = c
                 if a.status != 0 or b.status != 0:
+                    for later in checkpoints[k:]:
+                        stopped[later] += 1
                     break
                 xa, _ = i32.get_state()
                 xb, _ = i64.get_state()
@@ -127,13 +132,14 @@ def precision_study(n: int = 1_000_000, r: float = 8.0, seeds=range(8),
     finally:
         i32.close()
         i64.close()
-    out = {"n": n, "m": f.m, "seeds": len(list(seeds)), "max_steps": max_steps, "checkpoints": {}}
+    out = {"n": n, "m": f.m, "r": r, "seeds": len(list(seeds)), "max_steps": max_steps,
+           "checkpoints": {}}
     for c in checkpoints:
+        row = {"runs": len(errs[c]["dv"]), "stopped_before": stopped[c]}
         if errs[c]["dv"]:
-            out["checkpoints"][str(c)] = {"runs": len(errs[c]["dv"]),
-                                          "max_abs_dv": max(errs[c]["dv"]),
-                                          "max_abs_dxl": max(errs[c]["dxl"]),
-                                          "median_max_abs_dv": float(np.median(errs[c]["dv"]))}
+            row.update(max_abs_dv=max(errs[c]["dv"]), max_abs_dxl=max(errs[c]["dxl"]),
+                       median_max_abs_dv=float(np.median(errs[c]["dv"])))
+        out["checkpoints"][str(c)] = row
     for name in ("fp32", "fp64"):
         solved = [st for ok, st in res[name] if ok]
         out[name] = {"solve_rate": len(solved) / max(1, len(res[name])),
