@@ -99,27 +99,41 @@ __device__ __forceinline__ void advance_memory(T& Xs, T& Xl, T Cp, T alpha_c,
 template <class T>
 __device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
 
+// x, or -x when `neg`: equals mul(-1, x) bit for bit (a sign flip is exact).
+template <class T>
+__device__ __forceinline__ T neg_if(T x, bool neg) { return neg ? -x : x; }
+
 // 3-literal clause (dynex.cc:371-418).  v*: raw voltages.  Returns C_m.
+//
+// Evaluated with exact rewrites of the reference's operations (q_i = +-1 is the literal's
+// sign, c_i the clamped voltage, a_i = 1 - q_i c_i):
+//   q_i c_i            = c_i with its sign flipped for a negative literal;
+//   v_i has the literal's strict sign  <=>  q_i c_i > 0;
+//   h_i = a_i / 2 is exact (a_i = 0 or a_i >= 2^-24), so min(a) / 2 = min(h), the test
+//   C == a_i / 2 is C == h_i, and min_{j != i}(a_j) q_i / 2 = q_i min_{j != i}(h_j);
+//   (q_i - c_i) / 2 = q_i h_i, because q_i - c_i = q_i a_i exactly (round-to-nearest is
+//   symmetric under negation).
+// Every value, NaN propagation included, is the one the literal formula gives.
 template <class T>
 __device__ __forceinline__ T clause3(int l0, int l1, int l2, T v0, T v1, T v2, T Xs, T Xl,
                                      const ClauseConsts<T>& k, T& u0, T& u1, T& u2,
                                      bool& strict_sat) {
   const T one = T(1), half = T(0.5), zero = T(0);
-  strict_sat = (v0 > zero && l0 > 0) || (v0 < zero && l0 < 0) || (v1 > zero && l1 > 0) ||
-               (v1 < zero && l1 < 0) || (v2 > zero && l2 > 0) || (v2 < zero && l2 < 0);
+  const bool n0 = l0 < 0, n1 = l1 < 0, n2 = l2 < 0;
   const T c0 = clampv(v0, -one, one), c1 = clampv(v1, -one, one), c2 = clampv(v2, -one, one);
-  const T q0 = l0 > 0 ? one : -one, q1 = l1 > 0 ? one : -one, q2 = l2 > 0 ? one : -one;
-  const T a0 = sub(one, mul(q0, c0)), a1 = sub(one, mul(q1, c1)), a2 = sub(one, mul(q2, c2));
-  const T m12 = tmin(a1, a2), m02 = tmin(a0, a2), m01 = tmin(a0, a1);
-  const T C = mul(tmin(a0, m12), half);
+  const T p0 = neg_if(c0, n0), p1 = neg_if(c1, n1), p2 = neg_if(c2, n2);
+  strict_sat = p0 > zero || p1 > zero || p2 > zero;
+  const T h0 = mul(sub(one, p0), half), h1 = mul(sub(one, p1), half),
+          h2 = mul(sub(one, p2), half);
+  const T m12 = tmin(h1, h2), m02 = tmin(h0, h2), m01 = tmin(h0, h1);
+  const T C = tmin(h0, m12);
   const T xs = clampv(Xs, zero, one), xl = clampv(Xl, one, k.xlmax);
   const T xlxs = mul(xl, xs);
   const T rfac = mul(add(one, mul(k.zeta, xl)), sub(one, xs));
-  const T g0 = mul(mul(q0, m12), half), g1 = mul(mul(q1, m02), half),
-          g2 = mul(mul(q2, m01), half);
-  const T r0 = (C == mul(a0, half)) ? mul(sub(q0, c0), half) : zero;
-  const T r1 = (C == mul(a1, half)) ? mul(sub(q1, c1), half) : zero;
-  const T r2 = (C == mul(a2, half)) ? mul(sub(q2, c2), half) : zero;
+  const T g0 = neg_if(m12, n0), g1 = neg_if(m02, n1), g2 = neg_if(m01, n2);
+  const T r0 = (C == h0) ? neg_if(h0, n0) : zero;
+  const T r1 = (C == h1) ? neg_if(h1, n1) : zero;
+  const T r2 = (C == h2) ? neg_if(h2, n2) : zero;
   u0 = add(mul(xlxs, g0), mul(rfac, r0));
   u1 = add(mul(xlxs, g1), mul(rfac, r1));
   u2 = add(mul(xlxs, g2), mul(rfac, r2));

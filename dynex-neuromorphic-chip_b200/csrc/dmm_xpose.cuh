@@ -11,16 +11,18 @@
 //      written to a shared staging area grouped by destination variable tile (one chunk
 //      per variable tile, padded to 8 entries = one sector) and the area is written to
 //      global memory with 16-byte stores.
-//   B  a variable tile copies its chunk of every clause tile (contiguous, sector-aligned)
-//      with 4-byte asynchronous copies straight to each value's variable-major position
-//      in shared memory, then reduces each variable from there.
+//   B  a variable tile loads its chunk of every clause tile (contiguous, sector-aligned)
+//      with 16-byte loads and stores each value to its variable-major position in shared
+//      memory, then reduces each variable from there; the lanes of a variable's group form
+//      one Euler candidate each.
 //
 // Grid barriers are split (arrive ... wait) so that loads that do not depend on the other
-// blocks (the voltages of phase B's variables) are in flight during the wait.
+// blocks (the voltages of phase B's variables; at barrier 2 the step's phase-A counts) are
+// in flight during the wait.
 // Barrier 2 carries the step decision: a block arrives by adding 1 << (12 k) to the step's
 // arrival word, k = the largest trial index of its variables, so that the word that ends
 // the wait also holds the step's largest trial index.  The step's unsatisfied count and
-// strict-sign failures (complete at barrier 1) are read during phase B.  Every block applies
+// strict-sign failures (complete at barrier 1) are read during that wait.  Every block applies
 // the decision to its own copy of the control state; block 0 writes it for the host.
 //
 // Every clause value and every per-variable sum is computed from the same operands in the
@@ -131,8 +133,7 @@ __global__ void __launch_bounds__(NT, 1)
   __shared__ int dbeg, dcnt, ubase, ulen, bbeg, blen;
   __shared__ double red[NT / 32];
   __shared__ int cnt[2][NT / 32];
-  __shared__ int s_ok, s_loc, s_vfail;
-  __shared__ unsigned long long s_energy;
+  __shared__ int s_ok;
   const XpLayout LY = xp_layout(P.xsv_cap, P.xbk_cap, P.xtv_cap);
   T* sV = reinterpret_cast<T*>(staged_smem + LY.sv);
   T* stage = reinterpret_cast<T*>(staged_smem + LY.bk);  // phase A
@@ -301,9 +302,6 @@ __global__ void __launch_bounds__(NT, 1)
     target += gridDim.x + (s == 0 ? P.barrier_extra : 0);
     T cv = T(0);
     const int nv = has_v ? vtile.count : 0, v0 = has_v ? vtile.begin : 0;
-    const uint32_t* __restrict__ xd2 =
-        reinterpret_cast<const uint32_t*>(P.xdst + bbeg);  // positions, two per word
-    const int nb2 = blen / 2;
     if (has_v) {
       if (tid < nv) cv = V[v0 + tid];  // V(step) of the tile's variables
     }
@@ -327,38 +325,40 @@ __global__ void __launch_bounds__(NT, 1)
     }
     trace_stamp(P, s, 4);
 
-    // the step's counts of phase A, used by the decision after barrier 2
-    if (tid == 0) {
-      const volatile StepAcc* A = acc;
-      s_loc = A->loc;
-      s_vfail = A->vfail;
-      if (b == 0) {
-        s_energy = A->energy;
-        // every block has passed barrier 2 of step s-1, the last reader of the other slot
-        StepAcc* z = P.acc2 + ((s + 1) & 1);
-        z->loc = 0;
-        z->vfail = 0;
-        z->kmax = 0;
-        z->energy = 0ull;
-        z->arrive = 0ull;
-      }
+    // every block has finished step s-1, whose barrier 2 read the other slot last
+    if (tid == 0 && b == 0) {
+      StepAcc* z = P.acc2 + ((s + 1) & 1);
+      z->loc = 0;
+      z->vfail = 0;
+      z->kmax = 0;
+      z->energy = 0ull;
+      z->arrive = 0ull;
     }
     trace_stamp(P, s, 5);
 
     // ---- phase B
     if (has_v) {
-      auto issue = [&](int q, uint32_t word) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const unsigned pos = h ? (word >> 16) : (word & 0xffffu);
-          const int p = 2 * q + h;
-          if (pos != kXpPad) cp_async4(bucket + pos, P.ux + s_src8[p >> 3] + (p & 7));
+      // the tile's chunks, 4 values per thread and pass: one 16-byte load of a chunk (L2,
+      // written by other blocks this step) and four shared stores to the values'
+      // variable-major positions
+      {
+        const uint2* __restrict__ xd4 = reinterpret_cast<const uint2*>(P.xdst + bbeg);
+        const int nb4 = blen / 4;
+#pragma unroll 4
+        for (int q = tid; q < nb4; q += NT) {
+          const int p = 4 * q;
+          const float4 val =
+              __ldcg(reinterpret_cast<const float4*>(P.ux + s_src8[p >> 3] + (p & 7)));
+          const uint2 w = __ldg(xd4 + q);
+          const unsigned d0 = w.x & 0xffffu, d1 = w.x >> 16, d2 = w.y & 0xffffu, d3 = w.y >> 16;
+          if (d0 != kXpPad) bucket[d0] = val.x;
+          if (d1 != kXpPad) bucket[d1] = val.y;
+          if (d2 != kXpPad) bucket[d2] = val.z;
+          if (d3 != kXpPad) bucket[d3] = val.w;
         }
-      };
-      for (int q = tid; q < nb2; q += NT) issue(q, __ldg(xd2 + q));
+      }
       if (tid < nv) s_cur[tid] = cv;
       for (int i = tid + NT; i < nv; i += NT) s_cur[i] = V[v0 + i];
-      cp_async_wait_all();
       __syncthreads();
       trace_stamp(P, s, 6);
       T* __restrict__ nxt = P.cand + (int64_t)((set ^ 1) * kTrials) * P.var_cap + I.var0;
@@ -374,7 +374,25 @@ __global__ void __launch_bounds__(NT, 1)
           s1 = s_vend[i + 1];
         }
         const T dv = tree_sum<T, G, true, int32_t>(bucket + s0, nullptr, s1 - s0, lane);
-        if (valid && lane == 0) {
+        if constexpr (G >= kTrials) {
+          // every lane of the group holds dv: lane k forms candidate k, and the group's
+          // first accepted trial is the lowest accepting lane (one ballot per warp)
+          bool acc_k = false;
+          if (valid && lane < kTrials) {
+            const T Vv = s_cur[i];
+            const int8_t un = s_unit[i];
+            const T h = lane == 0 ? T(0.125) : lane == 1 ? T(0.0625) : lane == 2 ? T(0.03125)
+                                                                            : T(0.015625);
+            T c = add(Vv, mul(h, dv));
+            if (un != 0) c = T(un);
+            c = clampv(c, T(-1), T(1));
+            nxt[(int64_t)lane * P.var_cap + v0 + i] = c;
+            acc_k = !(fabs((double)c - (double)Vv) >= 1.0);
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, acc_k);
+          const unsigned gb = (bal >> ((tid & 31) & ~(G - 1))) & ((1u << kTrials) - 1u);
+          if (valid) kmax_b = max(kmax_b, gb ? __ffs(gb) - 1 : kTrials);
+        } else if (valid && lane == 0) {
           const T Vv = s_cur[i];
           const int8_t un = s_unit[i];
           const int v = v0 + i;
@@ -406,6 +424,10 @@ __global__ void __launch_bounds__(NT, 1)
         for (int i = 0; i < NT / 32; i++) km = max(km, cnt[0][i]);
       }
       red_release64(&acc->arrive, 1ull << (kArriveBits * km));
+      // the step's counts of phase A (complete since barrier 1) load during the wait
+      const volatile StepAcc* A = acc;
+      const int loc = A->loc, vfail = A->vfail;
+      const unsigned long long energy = b == 0 ? A->energy : 0ull;
       int ok = 1, kmax = 0;
       long long it = 0;
       for (;;) {
@@ -429,7 +451,6 @@ __global__ void __launch_bounds__(NT, 1)
       }
       s_ok = ok;
       trace_stamp(P, s, 8);
-      const int loc = s_loc, vfail = s_vfail;
       const StepDecision d = decide(loc, vfail, kmax, lc.step, I.max_steps);
       if (b == 0) {
         InstCtrl* S = P.ctrl + ii;
@@ -447,7 +468,7 @@ __global__ void __launch_bounds__(NT, 1)
         }
         S->loc = loc;
         S->vfail = vfail;
-        S->energy = (double)s_energy * (1.0 / kEnergyUnitF32);
+        S->energy = (double)energy * (1.0 / kEnergyUnitF32);
         S->t = __dadd_rn(lc.t, d.ht);
         S->step = lc.step + 1;
         S->set = set ^ 1;

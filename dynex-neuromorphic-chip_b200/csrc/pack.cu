@@ -166,6 +166,7 @@ constexpr int kPersistThreads = 1024;  // block size of the cooperative step ker
 // FP64: 512 threads, so that the sorted sums and the clause code fit in registers without
 // spilling (measured 74.3 vs 76.4 us per n=100k step with 1024 threads)
 constexpr int kPersistThreads64 = 512;
+constexpr int kStagedThreads = 1024;  // block size of the staged form
 static int persist_threads(dmm_precision prec) {
   return prec == DMM_FP64 ? kPersistThreads64 : kPersistThreads;
 }
@@ -831,12 +832,12 @@ static const void* persist_fn_x(dmm_precision prec, int G) {
 // the staged form (FP32, single formula)
 static const void* staged_fn(int G) {
   switch (G) {
-    case 1: return (const void*)k_staged<1, kPersistThreads>;
-    case 2: return (const void*)k_staged<2, kPersistThreads>;
-    case 4: return (const void*)k_staged<4, kPersistThreads>;
-    case 8: return (const void*)k_staged<8, kPersistThreads>;
-    case 16: return (const void*)k_staged<16, kPersistThreads>;
-    default: return (const void*)k_staged<32, kPersistThreads>;
+    case 1: return (const void*)k_staged<1, kStagedThreads>;
+    case 2: return (const void*)k_staged<2, kStagedThreads>;
+    case 4: return (const void*)k_staged<4, kStagedThreads>;
+    case 8: return (const void*)k_staged<8, kStagedThreads>;
+    case 16: return (const void*)k_staged<16, kStagedThreads>;
+    default: return (const void*)k_staged<32, kStagedThreads>;
   }
 }
 
@@ -937,7 +938,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   const int bk_cap = std::max(h[2], 8);
   const int smem = xp_layout(sv_cap, bk_cap, TV).total;
   if (smem > kXpSmemMax) return DMM_OK;
-  if (occupancy_blocks(staged_fn(tun_.var_group), kPersistThreads, smem) * sms_ != grid_p_)
+  if (occupancy_blocks(staged_fn(tun_.var_group), kStagedThreads, smem) * sms_ != grid_p_)
     return DMM_OK;
   xsv_cap_ = sv_cap;
   xbk_cap_ = bk_cap;
@@ -1015,7 +1016,8 @@ dmm_status Pack::commit_tiles() {
     TV = block;
     if (live_list.size() == 1) {
       const int64_t n = inst_h_[live_list[0]].n;
-      TV = (int)std::max<int64_t>(kMinVarTile, ((n + spread - 1) / spread + 31) & ~int64_t(31));
+      // a multiple of 4 (not of a warp) so that every block gets a variable tile
+      TV = (int)std::max<int64_t>(kMinVarTile, ((n + spread - 1) / spread + 3) & ~int64_t(3));
     }
   }
   for (int32_t i : live_list) {
@@ -1085,8 +1087,9 @@ dmm_status Pack::launch_persist(int32_t nsteps) {
   const size_t smem = xp_active_ ? (size_t)xsmem_ : 0;
   if (smem)
     DMM_CUDA(cudaFuncSetAttribute(persist_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(persist_threads(prec_)), args,
-                                       smem, stream_));
+  const int block = xp_active_ ? kStagedThreads : persist_threads(prec_);
+  DMM_CUDA(cudaLaunchCooperativeKernel(persist_fn(), dim3(grid_p_), dim3(block), args, smem,
+                                       stream_));
   return DMM_OK;
 }
 
