@@ -389,7 +389,7 @@ def main():
     x0_p = torch.from_numpy(x0).pin_memory()
     pform = dmm.Formula(n, m, lits_p.numpy(), off_p.numpy(), form.max_occurrence)
     e2e_times, e2e_steps = [], []
-    for it in range(3 + 2):
+    for it in range(2 + 7):
         barrier()
         t0 = time.perf_counter()
         with dmm.Instance(pform, precision="fp32", device=local) as e:
