@@ -354,12 +354,7 @@ dmm_status dmm_batch_add(dmm_batch* b, const int32_t* lits, const int64_t* claus
   if (!b || !x0 || !index) return DMM_ERR_ARG;
   dmm::DeviceScope device_scope(b->pack->device());
   int32_t idx = -1;
-  DMM_TRY(b->pack->add(lits, clause_off, n, m, p, nullptr, max_steps, &idx));
-  dmm_status st = b->pack->set_state(idx, x0);
-  if (st != DMM_OK) {
-    b->pack->remove(idx);
-    return st;
-  }
+  DMM_TRY(b->pack->add(lits, clause_off, n, m, p, nullptr, max_steps, &idx, x0));
   *index = (int32_t)b->idx.size();
   b->idx.push_back(idx);
   b->m.push_back(m);

@@ -401,12 +401,14 @@ static __global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, in
 
 // Sorts each variable's slot list ascending (warp per variable, bitonic in shared
 // memory) so the CSR is independent of the scatter's atomic order.  Lists longer than
-// kSortCap are reported in `longv` for the host.
+// kSortCap are reported in `longv` (as var_base + v, at most cap entries; the count keeps
+// growing past cap) for the host.
 constexpr int kSortCap = 1024;
 static __global__ void __launch_bounds__(kThreads) k_sort_lists(const int32_t* __restrict__ vend, int n,
                                                          int32_t* __restrict__ vslot,
                                                          int32_t* __restrict__ longv,
-                                                         int32_t* __restrict__ nlong) {
+                                                         int32_t* __restrict__ nlong,
+                                                         int32_t var_base, int32_t cap) {
   extern __shared__ int32_t sm[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int32_t* buf = sm + w * kSortCap;
@@ -415,7 +417,10 @@ static __global__ void __launch_bounds__(kThreads) k_sort_lists(const int32_t* _
     const int d = s1 - s0;
     if (d <= 1) continue;
     if (d > kSortCap) {
-      if (lane == 0) longv[atomicAdd(nlong, 1)] = v;
+      if (lane == 0) {
+        const int pos = atomicAdd(nlong, 1);
+        if (pos < cap) longv[pos] = var_base + v;
+      }
       continue;
     }
     int N = 2;

@@ -98,8 +98,11 @@ class Pack {
   static int64_t bytes_per(dmm_precision prec, int64_t n, int64_t m, int64_t slots,
                            bool with_alpha_cm);
 
+  // x0 (n+2m doubles, optional): the instance starts runnable from this state, as after
+  // set_state, with no read-back of its control record.
   dmm_status add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
-                 const dmm_params* p, const double* alpha_cm, int32_t max_steps, int32_t* idx);
+                 const dmm_params* p, const double* alpha_cm, int32_t max_steps, int32_t* idx,
+                 const double* x0 = nullptr);
   dmm_status remove(int32_t idx);
   dmm_status set_params(int32_t idx, const dmm_params* p, const double* alpha_cm);
   dmm_status set_max_steps(int32_t idx, int32_t max_steps);
@@ -172,6 +175,9 @@ class Pack {
 
  private:
   dmm_status build_csr(const InstDesc& I, const int32_t* lits);
+  // sorts the slot lists longer than the device sorter (reported by the CSR builds since
+  // the last call); runs before the CSR is first used
+  dmm_status resolve_long_lists();
   dmm_status ensure_stage(int64_t doubles);
   dmm_status capture(int32_t steps);
   dmm_status launch_persist(int32_t nsteps);
@@ -187,6 +193,9 @@ class Pack {
   dmm_status upload_desc(int32_t idx);
   dmm_status write_ctrl(int32_t idx, const InstCtrl& c);
   dmm_status add_active(int32_t delta);
+  dmm_status upload_state(const InstDesc& I, const double* x);
+  static InstCtrl running_ctrl(const InstDesc& I, double t, int32_t step);
+  void retire(void* p);  // dev_free after this pack's queued work
 
   dmm_precision prec_;
   int dev_;
@@ -255,6 +264,8 @@ class Pack {
   int32_t* scan_tmp_ = nullptr;
   int64_t scan_tmp_cap_ = 0;
   int32_t* longv_d_ = nullptr;
+  int32_t longv_cap_ = 0;
+  bool long_pending_ = false;  // CSR builds since the last resolve_long_lists()
   double* stage_ = nullptr;
   int64_t stage_cap_ = 0;
   Tile* aux_ctiles_d_ = nullptr;

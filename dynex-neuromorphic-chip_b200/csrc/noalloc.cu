@@ -211,7 +211,7 @@ extern "C" dmm_status dmm_rhs3_f32_noalloc(const int32_t* lits, int32_t n, int32
   k_fill_start<<<grid, NA_THREADS, 0, st>>>(s->vend, n, s->fill);
   if (L > 0) k_scatter<<<grid, NA_THREADS, 0, st>>>(lits, L, s->fill, s->vslot);
   k_sort_lists<<<grid, kThreads, (kThreads / 32) * kSortCap * sizeof(int32_t), st>>>(
-      s->vend, n, s->vslot, s->longv, &s->counters[1]);
+      s->vend, n, s->vslot, s->longv, &s->counters[1], 0, NA_MAX_SLOTS / kSortCap + 2);
   DMM_CUDA(cudaGetLastError());
   int32_t nlong = 0;
   DMM_CUDA(cudaMemcpyAsync(&nlong, &s->counters[1], sizeof(int32_t), cudaMemcpyDeviceToHost, st));

@@ -259,7 +259,8 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   DMM_CUDA(dev_alloc(&active_d_, sizeof(int32_t)));
   DMM_CUDA(dev_alloc(&ring_d_, I * sizeof(int32_t)));
   DMM_CUDA(dev_alloc(&ring_tail_d_, 4 * sizeof(int32_t)));
-  DMM_CUDA(dev_alloc(&longv_d_, (S / kSortCap + 2) * sizeof(int32_t)));
+  longv_cap_ = (int32_t)(S / kSortCap + 2);
+  DMM_CUDA(dev_alloc(&longv_d_, longv_cap_ * sizeof(int32_t)));
   DMM_CUDA(dev_alloc(&live_d_, I * sizeof(int32_t)));
   DMM_CUDA(dev_alloc(&order_d_, I * sizeof(int32_t)));
   // [0] live formulas, [1] error flag, [3] k_inst queue; bytes 64..191: grid-barrier
@@ -343,7 +344,7 @@ int32_t Pack::free_insts() const {
 
 dmm_status Pack::ensure_stage(int64_t doubles) {
   if (doubles <= stage_cap_) return DMM_OK;
-  if (stage_) dev_free(stage_);
+  if (stage_) retire(stage_);
   stage_ = nullptr;
   stage_cap_ = 0;
   DMM_CUDA(dev_alloc(&stage_, doubles * sizeof(double)));
@@ -351,15 +352,26 @@ dmm_status Pack::ensure_stage(int64_t doubles) {
   return DMM_OK;
 }
 
+void Pack::retire(void* p) {
+  // the block may still be read by work queued on this pack's stream, and the cache can
+  // hand it to another stream at once
+  cudaStreamSynchronize(stream_);
+  dev_free(p);
+}
+
+// Small records travel as kernel arguments: stream-ordered, no host staging, no wait.
+__global__ void k_put_desc(InstDesc* dst, InstDesc d) { *dst = d; }
+__global__ void k_put_ctrl(InstCtrl* dst, InstCtrl c) { *dst = c; }
+
 dmm_status Pack::upload_desc(int32_t idx) {
-  DMM_CUDA(cudaMemcpyAsync(inst_d_ + idx, &inst_h_[idx], sizeof(InstDesc), cudaMemcpyHostToDevice,
-                           stream_));
+  k_put_desc<<<1, 1, 0, stream_>>>(inst_d_ + idx, inst_h_[idx]);
+  DMM_CUDA(cudaGetLastError());
   return DMM_OK;
 }
 
 dmm_status Pack::write_ctrl(int32_t idx, const InstCtrl& c) {
-  DMM_CUDA(cudaMemcpyAsync(ctrl_d_ + idx, &c, sizeof(InstCtrl), cudaMemcpyHostToDevice, stream_));
-  DMM_CUDA(cudaStreamSynchronize(stream_));
+  k_put_ctrl<<<1, 1, 0, stream_>>>(ctrl_d_ + idx, c);
+  DMM_CUDA(cudaGetLastError());
   return DMM_OK;
 }
 
@@ -418,7 +430,7 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
   }
   const int64_t need = n / (kThreads * 8) + 64;
   if (need > scan_tmp_cap_) {
-    if (scan_tmp_) dev_free(scan_tmp_);
+    if (scan_tmp_) retire(scan_tmp_);
     scan_tmp_ = nullptr;
     DMM_CUDA(dev_alloc(&scan_tmp_, need * 2 * sizeof(int32_t)));
     scan_tmp_cap_ = need;
@@ -430,35 +442,78 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
     k_scatter<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, fill, vsl);
     DMM_CUDA(cudaGetLastError());
   }
-  int32_t* nlong = ring_tail_d_ + 2;
-  DMM_CUDA(cudaMemsetAsync(nlong, 0, sizeof(int32_t), stream_));
+  // lists longer than the shared-memory sorter are appended to longv_d_ (count at
+  // ring_tail_d_[2]) and sorted by resolve_long_lists() before the CSR is first used, so
+  // that adding a formula needs no host synchronization
   const size_t smem = (kThreads / 32) * kSortCap * sizeof(int32_t);
-  k_sort_lists<<<blocks_for(n, kThreads / 32), kThreads, smem, stream_>>>(vend, n, vsl, longv_d_,
-                                                                          nlong);
+  k_sort_lists<<<blocks_for(n, kThreads / 32), kThreads, smem, stream_>>>(
+      vend, n, vsl, longv_d_, ring_tail_d_ + 2, (int32_t)I.var0, longv_cap_);
   DMM_CUDA(cudaGetLastError());
-  int32_t h_nlong = 0;
-  DMM_CUDA(cudaMemcpyAsync(&h_nlong, nlong, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
-  DMM_CUDA(cudaStreamSynchronize(stream_));
-  if (h_nlong > 0) {
-    // Lists longer than the shared-memory sorter: sorted on the host (setup only).
-    std::vector<int32_t> ids(h_nlong), ends(n);
-    DMM_CUDA(cudaMemcpy(ids.data(), longv_d_, h_nlong * 4, cudaMemcpyDeviceToHost));
-    DMM_CUDA(cudaMemcpy(ends.data(), vend, (size_t)n * 4, cudaMemcpyDeviceToHost));
-    std::vector<int32_t> seg;
-    for (int32_t v : ids) {
-      const int s0 = v > 0 ? ends[v - 1] : 0, s1 = ends[v];
-      seg.resize(s1 - s0);
-      DMM_CUDA(cudaMemcpy(seg.data(), vsl + s0, seg.size() * 4, cudaMemcpyDeviceToHost));
-      std::sort(seg.begin(), seg.end());
-      DMM_CUDA(cudaMemcpy(vsl + s0, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
-    }
-  }
+  long_pending_ = true;
   if (L > 0) {
     // variable-major position of every slot (the inverse of the sorted CSR)
     k_invert<<<blocks_for(L), kThreads, 0, stream_>>>(vsl, L, upos_ + I.slot0);
     DMM_CUDA(cudaGetLastError());
   }
   (void)lits_host;
+  return DMM_OK;
+}
+
+dmm_status Pack::resolve_long_lists() {
+  if (!long_pending_) return DMM_OK;
+  int32_t nlong = 0;
+  DMM_CUDA(cudaMemcpyAsync(&nlong, ring_tail_d_ + 2, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                           stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  if (nlong > 0) {
+    // sorted on the host (setup only); an entry whose formula was removed meanwhile is
+    // skipped, one whose range a later formula took is sorted again (harmless).  Past the
+    // list's capacity (formulas with long lists added and removed repeatedly before a
+    // commit) every long list of every live formula is taken.
+    std::vector<int32_t> ids;
+    if (nlong <= longv_cap_) {
+      ids.resize(nlong);
+      DMM_CUDA(cudaMemcpy(ids.data(), longv_d_, nlong * 4, cudaMemcpyDeviceToHost));
+    } else {
+      for (int32_t i = 0; i < (int32_t)live_.size(); i++) {
+        if (!live_[i]) continue;
+        const InstDesc& I = inst_h_[i];
+        std::vector<int32_t> ends(I.n);
+        DMM_CUDA(cudaMemcpy(ends.data(), vend_ + I.var0, (size_t)I.n * 4, cudaMemcpyDeviceToHost));
+        for (int32_t v = 0; v < I.n; v++)
+          if (ends[v] - (v > 0 ? ends[v - 1] : 0) > kSortCap) ids.push_back((int32_t)I.var0 + v);
+      }
+    }
+    std::vector<int32_t> redo;
+    std::vector<int32_t> seg;
+    for (int32_t g : ids) {
+      int32_t owner = -1;
+      for (int32_t i = 0; i < (int32_t)live_.size(); i++)
+        if (live_[i] && g >= inst_h_[i].var0 && g < inst_h_[i].var0 + inst_h_[i].n) owner = i;
+      if (owner < 0) continue;
+      const InstDesc& I = inst_h_[owner];
+      const int32_t v = g - (int32_t)I.var0;
+      int32_t e[2] = {0, 0};
+      if (v > 0)
+        DMM_CUDA(cudaMemcpy(e, vend_ + I.var0 + v - 1, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost));
+      else
+        DMM_CUDA(cudaMemcpy(e + 1, vend_ + I.var0, sizeof(int32_t), cudaMemcpyDeviceToHost));
+      int32_t* vsl = vslot_ + I.slot0;
+      seg.resize(e[1] - e[0]);
+      DMM_CUDA(cudaMemcpy(seg.data(), vsl + e[0], seg.size() * 4, cudaMemcpyDeviceToHost));
+      std::sort(seg.begin(), seg.end());
+      DMM_CUDA(cudaMemcpy(vsl + e[0], seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
+      if (std::find(redo.begin(), redo.end(), owner) == redo.end()) redo.push_back(owner);
+    }
+    for (int32_t i : redo) {
+      const InstDesc& I = inst_h_[i];
+      k_invert<<<blocks_for(I.nslots), kThreads, 0, stream_>>>(vslot_ + I.slot0, I.nslots,
+                                                               upos_ + I.slot0);
+      DMM_CUDA(cudaGetLastError());
+    }
+    DMM_CUDA(cudaMemsetAsync(ring_tail_d_ + 2, 0, sizeof(int32_t), stream_));
+  }
+  long_pending_ = false;
   return DMM_OK;
 }
 
@@ -481,6 +536,19 @@ static void fill_params(InstDesc& I, const dmm_params* p) {
   I.xl_max = effective_xl_max(p->xl_max, I.m);
 }
 
+// Copies from pageable host memory have read their source when cudaMemcpyAsync returns;
+// from page-locked memory they run later, so a call that copies from a caller's
+// page-locked buffer waits for its stream before returning (the caller may reuse it).
+static bool page_locked(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;  // unknown: treat as page-locked
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
 template <class T>
 static dmm_status upload_alpha(T* dst, const double* a, int32_t m, cudaStream_t s) {
   std::vector<T> h(m);
@@ -492,7 +560,7 @@ static dmm_status upload_alpha(T* dst, const double* a, int32_t m, cudaStream_t 
 
 dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
                      const dmm_params* p, const double* alpha_cm, int32_t max_steps,
-                     int32_t* idx_out) {
+                     int32_t* idx_out, const double* x0) {
   DMM_TRY(validate_shape(lits, clause_off, n, m));
   if (alpha_cm && !with_alpha_cm_) {
     set_error("this pack was created without per-clause alpha storage");
@@ -579,8 +647,25 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
   c.solved_step = -1;
   c.solved_t = -1.0;
   c.h_state = 0.125;
-  DMM_TRY(write_ctrl(idx, c));
+  if (x0) {
+    // runnable at once: the state set_state would upload, without reading the control
+    // record back (it is the one written here)
+    const dmm_status st = upload_state(I, x0);
+    if (st != DMM_OK) {
+      write_ctrl(idx, c);
+      var_alloc_.free(var0, n);
+      cls_alloc_.free(cls0, m);
+      slot_alloc_.free(slot0, L);
+      live_[idx] = 0;
+      return st;
+    }
+    DMM_TRY(write_ctrl(idx, running_ctrl(I, 0.0, 0)));
+    DMM_TRY(add_active(+1));
+  } else {
+    DMM_TRY(write_ctrl(idx, c));
+  }
   if (!fixed_grid_) graph_stale_ = true;
+  if (page_locked(lits) || page_locked(x0)) DMM_CUDA(cudaStreamSynchronize(stream_));
   *idx_out = idx;
   return DMM_OK;
 }
@@ -644,10 +729,23 @@ dmm_status Pack::set_state_at(int32_t idx, const double* x, double t, int32_t st
     return DMM_ERR_ARG;
   }
   const InstDesc& I = inst_h_[idx];
-  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
-  DMM_TRY(ensure_stage(3 * N));
   InstCtrl old;
   DMM_TRY(read_ctrl(idx, &old));
+  DMM_TRY(upload_state(I, x));
+  InstCtrl c = running_ctrl(I, t, step);
+  if (keep_best) {
+    c.best_loc = old.best_loc;
+    c.best_t = old.best_t;
+  }
+  if (old.done != 0) DMM_TRY(add_active(+1));
+  DMM_TRY(write_ctrl(idx, c));
+  if (page_locked(x)) DMM_CUDA(cudaStreamSynchronize(stream_));
+  return DMM_OK;
+}
+
+dmm_status Pack::upload_state(const InstDesc& I, const double* x) {
+  const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
+  DMM_TRY(ensure_stage(3 * N));
   DMM_CUDA(cudaMemcpyAsync(stage_, x, N * sizeof(double), cudaMemcpyHostToDevice, stream_));
   if (prec_ == DMM_FP64) {
     double* V = static_cast<double*>(cand_) + I.var0;
@@ -659,19 +757,21 @@ dmm_status Pack::set_state_at(int32_t idx, const double* x, double t, int32_t st
         stage_, I.n, I.m, V, static_cast<float*>(Xs_) + I.cls0, static_cast<float*>(Xl_) + I.cls0);
   }
   DMM_CUDA(cudaGetLastError());
+  return DMM_OK;
+}
+
+InstCtrl Pack::running_ctrl(const InstDesc& I, double t, int32_t step) {
   InstCtrl c{};
   c.done = 0;
   c.step = step;
   c.t = t;
   c.loc = I.m;
-  c.best_loc = keep_best ? old.best_loc : I.m;
-  c.best_t = keep_best ? old.best_t : 0.0;
+  c.best_loc = I.m;
+  c.best_t = 0.0;
   c.solved_step = -1;
   c.solved_t = -1.0;
   c.h_state = 0.125;
-  if (old.done != 0) DMM_TRY(add_active(+1));
-  DMM_TRY(write_ctrl(idx, c));
-  return DMM_OK;
+  return c;
 }
 
 dmm_status Pack::get_state(int32_t idx, double* x, double* t) {
@@ -889,7 +989,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   for (int i = 0; i < kXpBufs; i++) {
     const int64_t want = std::max<int64_t>(bytes[i], 16);
     if (want > xbuf_cap_[i]) {
-      if (xbuf_[i]) dev_free(xbuf_[i]);
+      if (xbuf_[i]) retire(xbuf_[i]);
       xbuf_[i] = nullptr;
       xbuf_cap_[i] = 0;
       DMM_CUDA(dev_alloc(&xbuf_[i], want));
@@ -951,6 +1051,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
 }
 
 dmm_status Pack::commit_tiles() {
+  DMM_TRY(resolve_long_lists());
   xp_active_ = false;
   one_active_ = false;
   ctiles_h_.clear();
@@ -1201,7 +1302,7 @@ dmm_status Pack::launch_steps(int32_t nsteps) {
 
 dmm_status Pack::ensure_flush(int64_t flush_bytes) {
   if (flush_bytes > flush_cap_) {
-    if (flush_) dev_free(flush_);
+    if (flush_) retire(flush_);
     flush_ = nullptr;
     DMM_CUDA(dev_alloc(&flush_, flush_bytes));
     flush_cap_ = flush_bytes;
@@ -1236,7 +1337,8 @@ dmm_status Pack::preload_kernels() {
   std::vector<const void*> fns = {
       persist_fn_x<false>(prec_, G), (const void*)k_count, (const void*)k_scan_block,
       (const void*)k_scan_add, (const void*)k_fill_start, (const void*)k_scatter,
-      (const void*)k_sort_lists, (const void*)k_invert, (const void*)k_active_add};
+      (const void*)k_sort_lists, (const void*)k_invert, (const void*)k_active_add,
+      (const void*)k_put_desc,   (const void*)k_put_ctrl};
   if (prec_ == DMM_FP64) {
     fns.push_back((const void*)k_set_state<double>);
     fns.push_back((const void*)k_get_state<double>);
@@ -1282,7 +1384,7 @@ dmm_status Pack::trace_phases(int32_t nsteps, double* out) {
   const int64_t half = (int64_t)nsteps * K * grid_p_;
   const int64_t need = 2 * half;  // timer stamps, then clock counts
   if (need > trace_cap_) {
-    if (trace_) dev_free(trace_);
+    if (trace_) retire(trace_);
     trace_ = nullptr;
     DMM_CUDA(dev_alloc(&trace_, need * sizeof(long long)));
     trace_cap_ = need;
@@ -1343,7 +1445,7 @@ dmm_status Pack::trace_phases(int32_t nsteps, double* out) {
 dmm_status Pack::profile_steps(int32_t nsteps, int64_t flush_bytes, StepTimes* t) {
   DMM_CUDA(cudaSetDevice(dev_));
   if (flush_bytes > flush_cap_) {
-    if (flush_) dev_free(flush_);
+    if (flush_) retire(flush_);
     flush_ = nullptr;
     DMM_CUDA(dev_alloc(&flush_, flush_bytes));
     flush_cap_ = flush_bytes;
@@ -1461,6 +1563,7 @@ dmm_status Pack::sync() {
 
 dmm_status Pack::rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, double* energy) {
   if (!live(idx) || !x || !dxdt) return DMM_ERR_ARG;
+  DMM_TRY(resolve_long_lists());
   DMM_TRY(set_state(idx, x));
   const InstDesc& I = inst_h_[idx];
   const int64_t N = (int64_t)I.n + 2 * (int64_t)I.m;
@@ -1472,8 +1575,8 @@ dmm_status Pack::rhs(int32_t idx, const double* x, double* dxdt, int32_t* loc, d
   for (int32_t b = 0; b < I.n; b += TV) vt.push_back(Tile{idx, b, std::min(TV, I.n - b), 0});
   const int64_t need = std::max<int64_t>(std::max(ct.size(), vt.size()), 1);
   if (need > aux_cap_) {
-    if (aux_ctiles_d_) dev_free(aux_ctiles_d_);
-    if (aux_vtiles_d_) dev_free(aux_vtiles_d_);
+    if (aux_ctiles_d_) retire(aux_ctiles_d_);
+    if (aux_vtiles_d_) retire(aux_vtiles_d_);
     aux_ctiles_d_ = aux_vtiles_d_ = nullptr;
     DMM_CUDA(dev_alloc(&aux_ctiles_d_, need * sizeof(Tile)));
     DMM_CUDA(dev_alloc(&aux_vtiles_d_, need * sizeof(Tile)));

@@ -180,19 +180,18 @@ static dmm_status admit(dmm_server* s, bool* changed) {
       ++it;
       continue;
     }
+    if (r.x0.empty()) {
+      r.x0.resize((size_t)r.n + 2 * (size_t)r.m);
+      DMM_TRY(dmm_initial_state_uniform(r.lits.data(), r.off.data(), r.n, r.m, r.seed, r.x0.data()));
+    }
     int32_t idx = -1;
     dmm_status st = s->pack->add(r.lits.data(), r.off.data(), r.n, r.m, &r.p, nullptr,
-                                 r.max_steps, &idx);
+                                 r.max_steps, &idx, r.x0.data());
     if (st == DMM_ERR_BUDGET) {  // fragmented arena: try again after retirements
       ++it;
       continue;
     }
     DMM_TRY(st);
-    if (r.x0.empty()) {
-      r.x0.resize((size_t)r.n + 2 * (size_t)r.m);
-      DMM_TRY(dmm_initial_state_uniform(r.lits.data(), r.off.data(), r.n, r.m, r.seed, r.x0.data()));
-    }
-    DMM_TRY(s->pack->set_state(idx, r.x0.data()));
     Resident res;
     res.ticket = r.ticket;
     res.n = r.n;
