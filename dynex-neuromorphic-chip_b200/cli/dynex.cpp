@@ -3,7 +3,7 @@
 //
 //   dynex -i file.cnf [-l seed] [-w replicas] [-u walltime] [-z maxsteps]
 //         [-c alpha] [-b beta] [-n gamma] [-h delta] [-j epsilon] [-k zeta] [-m xl_max]
-//         [-q 0|1] [-p 0|1] [-P fp64|fp32] [-D device]
+//         [-q 0|1] [-p 0|1] [-P fp64|fp32] [-D device] [-L 0|1] [-S 0|1]
 //
 // Defaults follow the reference (FP64 arithmetic, seed 0, one replica); with them the
 // reported step count, T and assignment equal the reference's.  -P fp32 selects the
@@ -12,7 +12,10 @@
 // that solves at the lowest step wins.  -p 1 runs the reference's alpha heuristic every
 // 10^4 steps (one replica).  Options of the reference that select modes outside the
 // default integrator (-o, -t, -e, ...) are accepted and reported as unsupported when they
-// ask for anything but the default.
+// ask for anything but the default.  -S 1 writes the final state of the reported replica
+// to <cnf>.assignment.txt in the reference's checkpoint format (dynex.cc:2131-2135); -L 1
+// starts every replica from that file, at its time t, as the reference's load_assignment
+// does (dynex.cc:2521-2532, 2688-2692; a compile-time switch there).
 #include <getopt.h>
 #include <unistd.h>
 
@@ -39,8 +42,20 @@ struct Opts {
   bool heuristics = false;
   dmm_precision prec = DMM_FP64;
   int device = 0;
+  bool load_state = false;  // -L: start from <cnf>.assignment.txt
+  bool save_state = false;  // -S: write the final state to <cnf>.assignment.txt
   dmm_params p{};
 };
+
+// V of unit-clause variables pinned to the clause's sign, the last unit clause of a
+// variable winning (dynex.cc:2459-2469, applied to every initial state at :2694-2698).
+void pin_units(const dmm_cnf* cnf, std::vector<double>& x) {
+  for (int32_t c = 0; c < cnf->m; c++)
+    if (cnf->clause_off[c + 1] - cnf->clause_off[c] == 1) {
+      const int32_t l = cnf->lits[cnf->clause_off[c]];
+      x[std::abs(l) - 1] = l > 0 ? 1.0 : -1.0;
+    }
+}
 
 constexpr int kHeuristicEvery = 10000;  // dynex.cc:1430
 
@@ -100,7 +115,9 @@ void usage(const char* argv0) {
       "c   -m int      Xl bound factor (bound = factor * m)\n"
       "c   -q 0|1      quiet\n"
       "c   -P fp64|fp32  arithmetic (default fp64, the reference's)\n"
-      "c   -D int      CUDA device\n");
+      "c   -D int      CUDA device\n"
+      "c   -L 0|1      start from <file>.assignment.txt (V, Xs, Xl and t)\n"
+      "c   -S 0|1      write the final state to <file>.assignment.txt\n");
 }
 
 bool fail(dmm_status st, const char* what) {
@@ -119,7 +136,7 @@ int main(int argc, char** argv) {
   Opts o;
   dmm_params_default(&o.p);
   int c;
-  while ((c = getopt(argc, argv, "i:l:w:u:z:c:b:n:h:j:k:m:q:P:D:o:t:p:e:f:g:r:v:x:y:d:a:s:")) != -1) {
+  while ((c = getopt(argc, argv, "i:l:w:u:z:c:b:n:h:j:k:m:q:P:D:L:S:o:t:p:e:f:g:r:v:x:y:d:a:s:")) != -1) {
     const char* a = optarg;
     if (a && a[0] == '=') a++;  // the reference accepts -x=value (dynex.cc:2208)
     switch (c) {
@@ -138,6 +155,8 @@ int main(int argc, char** argv) {
       case 'q': o.quiet = std::atoi(a) != 0; break;
       case 'P': o.prec = std::strcmp(a, "fp32") == 0 ? DMM_FP32 : DMM_FP64; break;
       case 'D': o.device = std::atoi(a); break;
+      case 'L': o.load_state = std::atoi(a) != 0; break;
+      case 'S': o.save_state = std::atoi(a) != 0; break;
       case 'o':
         if (std::atoi(a) != 6) std::fprintf(stderr, "c -o %s: only the default integrator (6) is available\n", a);
         break;
@@ -179,6 +198,23 @@ int main(int argc, char** argv) {
   }
   const int64_t N = (int64_t)n + 2 * (int64_t)m;
   std::vector<double> x(N);
+  const std::string state_file = o.input + ".assignment.txt";
+  // -L: the checkpoint replaces every replica's initial state; read as the reference's
+  // loader reads it (each value through a float)
+  std::vector<double> x_loaded;
+  double t_loaded = 0.0;
+  if (o.load_state) {
+    x_loaded.resize(N);
+    if (dmm_state_read(state_file.c_str(), n, m, 1, x_loaded.data(), &t_loaded) == DMM_OK) {
+      pin_units(cnf, x_loaded);
+      if (!o.quiet)
+        std::printf("c ASSIGNMENT %s LOADED, WILL START AT t=%g\n", state_file.c_str(), t_loaded);
+    } else {
+      std::fprintf(stderr, "c -L: %s not loaded (%s)\n", state_file.c_str(), dmm_last_error());
+      x_loaded.clear();
+      t_loaded = 0.0;
+    }
+  }
   const double t0 = now_s();
   dmm_report rep{};
   std::vector<int8_t> pre(n), post(n);
@@ -192,7 +228,9 @@ int main(int argc, char** argv) {
         fail(dmm_initial_state_reference(cnf->lits, cnf->clause_off, n, m, o.seed, 0, x.data(), &div),
              "initial state") ||
         fail(dmm_instance_set_params(inst, &o.p, nullptr), "parameters") ||
-        fail(dmm_instance_set_state(inst, x.data()), "state")) {
+        fail(x_loaded.empty() ? dmm_instance_set_state(inst, x.data())
+                              : dmm_instance_set_state_at(inst, x_loaded.data(), t_loaded, 0),
+             "state")) {
       dmm_instance_destroy(inst);
       dmm_cnf_free(cnf);
       return EXIT_FAILURE;
@@ -243,8 +281,12 @@ int main(int argc, char** argv) {
       return EXIT_FAILURE;
     }
     solved = rep.status == DMM_SOLVED;
+    double t_end = 0.0;
     if (fail(dmm_instance_assignment(inst, solved ? pre.data() : nullptr, post.data()),
-             "assignment")) {
+             "assignment") ||
+        (o.save_state && (fail(dmm_instance_get_state(inst, x.data(), &t_end), "state") ||
+                          fail(dmm_state_write(state_file.c_str(), x.data(), n, m, t_end),
+                               "writing the state")))) {
       dmm_instance_destroy(inst);
       dmm_cnf_free(cnf);
       return EXIT_FAILURE;
@@ -267,8 +309,12 @@ int main(int argc, char** argv) {
                "initial state"))
         return EXIT_FAILURE;
       pr.alpha = o.p.alpha / div;  // dynex.cc:2657
-      if (fail(dmm_batch_add(b, cnf->lits, cnf->clause_off, n, m, &pr, x.data(), o.max_steps, &idx),
+      const double* xr = x_loaded.empty() ? x.data() : x_loaded.data();
+      if (fail(dmm_batch_add(b, cnf->lits, cnf->clause_off, n, m, &pr, xr, o.max_steps, &idx),
                "adding a replica"))
+        return EXIT_FAILURE;
+      if (!x_loaded.empty() && t_loaded != 0.0 &&
+          fail(dmm_batch_set_state_at(b, idx, xr, t_loaded, 0), "state"))
         return EXIT_FAILURE;
     }
     if (!o.quiet) std::printf("c [*] STARTING ODE ON %d REPLICAS...\n", R);
@@ -290,6 +336,11 @@ int main(int argc, char** argv) {
     winner = best;
     solved = rep.status == DMM_SOLVED;
     dmm_batch_assignment(b, best, solved ? pre.data() : nullptr, post.data());
+    double t_end = 0.0;
+    if (o.save_state && (fail(dmm_batch_state(b, best, x.data(), &t_end), "state") ||
+                         fail(dmm_state_write(state_file.c_str(), x.data(), n, m, t_end),
+                              "writing the state")))
+      return EXIT_FAILURE;
     dmm_batch_destroy(b);
   }
   const double spent = now_s() - t0;

@@ -444,4 +444,12 @@ dmm_status dmm_batch_state(dmm_batch* b, int32_t index, double* x, double* t) {
   return b->pack->get_state(b->idx[index], x, t);
 }
 
+dmm_status dmm_batch_set_state_at(dmm_batch* b, int32_t index, const double* x, double t,
+                                  int32_t step) {
+  dmm::clear_error();
+  if (!b || !x || index < 0 || index >= (int32_t)b->idx.size() || step < 0) return DMM_ERR_ARG;
+  dmm::DeviceScope device_scope(b->pack->device());
+  return b->pack->set_state_at(b->idx[index], x, t, step, false);
+}
+
 }  // extern "C"

@@ -1,6 +1,7 @@
 // Host-side formula handling: DIMACS reader/writer, planted generator, strict-sign
 // checker and initial states.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -239,6 +240,55 @@ dmm_status dmm_cnf_write(const dmm_cnf* c, const char* path, const int8_t* plant
   }
   const bool ok = std::fclose(f) == 0;
   return ok ? DMM_OK : DMM_ERR_IO;
+}
+
+dmm_status dmm_state_write(const char* path, const double* x, int32_t n, int32_t m, double t) {
+  clear_error();
+  if (!path || !x || n < 0 || m < 0) return DMM_ERR_ARG;
+  FILE* f = std::fopen(path, "w");
+  if (!f) {
+    set_error("cannot write %s", path);
+    return DMM_ERR_IO;
+  }
+  const int64_t N = (int64_t)n + 2 * (int64_t)m;
+  for (int64_t j = 0; j < N; j++) std::fprintf(f, "%.15f, ", x[j]);
+  std::fprintf(f, "%.15f ", t);
+  const bool ok = std::fclose(f) == 0;
+  if (!ok) set_error("writing %s failed", path);
+  return ok ? DMM_OK : DMM_ERR_IO;
+}
+
+dmm_status dmm_state_read(const char* path, int32_t n, int32_t m, int32_t reference_rounding,
+                          double* x, double* t) {
+  clear_error();
+  if (!path || !x || !t || n < 0 || m < 0) return DMM_ERR_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    set_error("cannot read %s", path);
+    return DMM_ERR_IO;
+  }
+  std::string text;
+  char buf[1 << 16];
+  size_t got;
+  while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+  std::fclose(f);
+  const int64_t N = (int64_t)n + 2 * (int64_t)m;
+  const char* p = text.c_str();
+  for (int64_t k = 0; k <= N; k++) {
+    while (*p == ',' || std::isspace((unsigned char)*p)) p++;
+    char* end = nullptr;
+    // the reference reads each value with fscanf("%f") into a float
+    const double v = reference_rounding ? (double)std::strtof(p, &end) : std::strtod(p, &end);
+    if (end == p) {
+      set_error("%s: %lld numbers where the state needs %lld (n + 2m values and t)", path,
+                (long long)k, (long long)(N + 1));
+      return DMM_ERR_PARSE;
+    }
+    p = end;
+    if (k < N) x[k] = v;
+    else *t = v;
+  }
+  return DMM_OK;
 }
 
 dmm_status dmm_cnf_generate_planted(int32_t n, int32_t m, double p0, double p1, uint64_t seed,

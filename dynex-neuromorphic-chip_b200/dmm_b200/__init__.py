@@ -7,7 +7,8 @@ from ._lib import (CANCELLED, RUNNING, SOLVED, STEP_LIMIT, TIME_LIMIT, DmmError,
                    default_params, lib)
 from .batch import Batch
 from .cnf import (Formula, check_assignment, from_arrays, generate_planted,
-                  initial_state_reference, initial_state_uniform, read_cnf, write_cnf)
+                  initial_state_reference, initial_state_uniform, read_cnf, read_state,
+                  write_cnf, write_state)
 from .instance import Instance, Result
 from .server import Server
 
@@ -15,5 +16,5 @@ __all__ = [
     "Batch", "CANCELLED", "DmmError", "Formula", "Instance", "Params", "RUNNING", "Result",
     "SOLVED", "STEP_LIMIT", "Server", "TIME_LIMIT", "check_assignment", "default_params",
     "from_arrays", "generate_planted", "initial_state_reference", "initial_state_uniform", "lib",
-    "read_cnf", "write_cnf",
+    "read_cnf", "read_state", "write_cnf", "write_state",
 ]

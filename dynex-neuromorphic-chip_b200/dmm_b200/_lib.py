@@ -107,6 +107,8 @@ SIGNATURES = {
     "dmm_cnf_from_arrays": (_i32, [_pi32, _pi64, _i32, _i32, _P(_P(Cnf))]),
     "dmm_cnf_free": (None, [_P(Cnf)]),
     "dmm_cnf_write": (_i32, [_P(Cnf), ctypes.c_char_p, _pi8]),
+    "dmm_state_write": (_i32, [ctypes.c_char_p, _pd, _i32, _i32, _d]),
+    "dmm_state_read": (_i32, [ctypes.c_char_p, _i32, _i32, _i32, _pd, _pd]),
     "dmm_cnf_generate_planted": (_i32, [_i32, _i32, _d, _d, _u64, _P(_P(Cnf)), _pi8]),
     "dmm_check_assignment": (_i64, [_pi32, _pi64, _i32, _i32, _pi8]),
     "dmm_initial_state_reference": (_i32, [_pi32, _pi64, _i32, _i32, _i32, _i32, _pd, _pi32]),
@@ -141,6 +143,7 @@ SIGNATURES = {
     "dmm_batch_result": (_i32, [_vp, _i32, _P(Report), _pi8]),
     "dmm_batch_assignment": (_i32, [_vp, _i32, _pi8, _pi8]),
     "dmm_batch_state": (_i32, [_vp, _i32, _pd, _pd]),
+    "dmm_batch_set_state_at": (_i32, [_vp, _i32, _pd, _d, _i32]),
     "dmm_server_create": (_i32, [_P(ServerConfig), _P(_vp)]),
     "dmm_server_destroy": (None, [_vp]),
     "dmm_server_submit": (_i32, [_vp, _pi32, _pi64, _i32, _i32, _P(Params), _pd, _u64, _i32,

@@ -62,6 +62,25 @@ def write_cnf(f: Formula, path: str, planted=None) -> None:
     check(lib().dmm_cnf_write(ctypes.byref(c), path.encode(), ptr(pl, ctypes.c_int8)))
 
 
+def write_state(path: str, x, n: int, m: int, t: float) -> None:
+    """State checkpoint in the reference's `<cnf>.assignment.txt` format (dynex.cc:2131-2135):
+    the n + 2m values [V | Xs | Xl] as "%.15f, ", then t as "%.15f "."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.shape != (n + 2 * m,):
+        raise ValueError("x must have n + 2m entries")
+    check(lib().dmm_state_write(path.encode(), ptr(x, ctypes.c_double), int(n), int(m), float(t)))
+
+
+def read_state(path: str, n: int, m: int, reference_rounding: bool = False):
+    """(x, t) from a state checkpoint file (dynex.cc:2521-2532); reference_rounding rounds
+    every value to float as the reference's loader does."""
+    x = np.zeros(n + 2 * m, dtype=np.float64)
+    t = ctypes.c_double()
+    check(lib().dmm_state_read(path.encode(), int(n), int(m), int(bool(reference_rounding)),
+                               ptr(x, ctypes.c_double), ctypes.byref(t)))
+    return x, t.value
+
+
 def generate_planted(n: int, m: int, p0: float = 0.08, p1: float = 0.46, seed: int = 0):
     """Planted 3-SAT: (Formula, planted +1/-1 assignment).  p0/p1: probability that 3 / 1
     literals of a clause agree with the planted assignment (else 2)."""

@@ -165,6 +165,17 @@ dmm_status dmm_cnf_generate_planted(int32_t n, int32_t m, double p0, double p1, 
  * matches assign[var] (+1 true, -1 false, 0 matches nothing).  -1 on bad arguments. */
 int64_t dmm_check_assignment(const int32_t* lits, const int64_t* clause_off, int32_t m,
                              int32_t n, const int8_t* assign);
+/* State checkpoint file in the reference's `<cnf>.assignment.txt` format (writer
+ * dynex.cc:2131-2135): the n + 2m state values [V | Xs | Xl] each printed as "%.15f, ",
+ * then the simulated time t as "%.15f ". */
+dmm_status dmm_state_write(const char* path, const double* x, int32_t n, int32_t m, double t);
+/* Reads that format (loader dynex.cc:2521-2532): n + 2m values, then t; values may be
+ * separated by commas and white space, anything after t is ignored.  reference_rounding = 1
+ * rounds every value to float, as the reference's loader does (it reads each one with "%f"
+ * into a float); 0 keeps the printed decimals in double precision.  DMM_ERR_IO when the
+ * file cannot be read, DMM_ERR_PARSE when it holds fewer than n + 2m + 1 numbers. */
+dmm_status dmm_state_read(const char* path, int32_t n, int32_t m, int32_t reference_rounding,
+                          double* x, double* t);
 /* Initial state of replica `replica` for CLI seed `seed` (dynex.cc:2635-2700, default flags).
  * x: n + 2m doubles.  *alpha_div receives the replica's alpha divisor (dynex.cc:2657). */
 dmm_status dmm_initial_state_reference(const int32_t* lits, const int64_t* clause_off,
@@ -314,7 +325,13 @@ dmm_status dmm_batch_run_until(dmm_batch* b, double wall_s, int32_t stop_after,
 dmm_status dmm_batch_result(dmm_batch* b, int32_t index, dmm_report* rep, int8_t* post);
 /* Assignments of one instance, as dmm_instance_assignment. */
 dmm_status dmm_batch_assignment(dmm_batch* b, int32_t index, int8_t* pre, int8_t* post);
+/* State of instance `index` in the reference layout [V | Xs | Xl] and its time t. */
 dmm_status dmm_batch_state(dmm_batch* b, int32_t index, double* x, double* t);
+/* Restarts instance `index` from state x at simulated time t after `step` accepted steps,
+ * as dmm_instance_set_state_at: a replica resumed from a checkpoint file starts at the
+ * file's t (the reference's t_init, dynex.cc:2531, 1229). */
+dmm_status dmm_batch_set_state_at(dmm_batch* b, int32_t index, const double* x, double t,
+                                  int32_t step);
 
 /* ---- continuous-batching server ------------------------------------------------------- */
 typedef struct dmm_server dmm_server;

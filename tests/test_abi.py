@@ -134,3 +134,35 @@ def test_formula_validation():
         dmm.from_arrays([1, 0, 2], [0, 3], 2)
     with pytest.raises(dmm.DmmError):
         dmm.from_arrays([1, 2], [0, 2], 0)
+
+
+def test_state_checkpoint_file_format(tmp_path):
+    """`<cnf>.assignment.txt` as the reference writes it (dynex.cc:2131-2135) and reads it
+    (dynex.cc:2521-2532, each value through a float)."""
+    n, m = 5, 3
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.uniform(-1, 1, n), rng.uniform(0, 1, m), rng.uniform(1, 900, m)])
+    x[0], x[1] = -0.0, 1.0
+    t = 1234.56789012345678
+    path = str(tmp_path / "f.cnf.assignment.txt")
+    dmm.write_state(path, x, n, m, t)
+    want = "".join("%.15f, " % v for v in x) + "%.15f " % t
+    assert open(path).read() == want
+    xd, td = dmm.read_state(path, n, m)
+    assert np.array_equal(xd, [float("%.15f" % v) for v in x]) and td == float("%.15f" % t)
+    xf, tf = dmm.read_state(path, n, m, reference_rounding=True)
+    assert np.array_equal(xf, np.float32(["%.15f" % v for v in x]).astype(np.float64))
+    assert tf == float(np.float32("%.15f" % t))
+    # separators as the reference's fscanf("%f, ") accepts them; trailing text is ignored
+    loose = tmp_path / "loose.txt"
+    loose.write_text("\n".join("%.6f ," % v for v in x) + "\n%.3f trailing" % t)
+    xl, tl = dmm.read_state(str(loose), n, m)
+    assert np.array_equal(xl, [float("%.6f" % v) for v in x]) and tl == float("%.3f" % t)
+    short = tmp_path / "short.txt"
+    short.write_text("".join("%.15f, " % v for v in x[:-1]))
+    with pytest.raises(dmm.DmmError) as e:
+        dmm.read_state(str(short), n, m)
+    assert e.value.name == "DMM_ERR_PARSE"
+    with pytest.raises(dmm.DmmError) as e:
+        dmm.read_state(str(tmp_path / "missing.txt"), n, m)
+    assert e.value.name == "DMM_ERR_IO"

@@ -100,3 +100,39 @@ def test_cli_alpha_heuristic_matches_reference(tmp_path, known_answers):
     assert out["steps"] == ka["steps"]
     assert out["T"] == pytest.approx(ka["T"], abs=1e-9)
     assert hashlib.sha256(np.array(out["v"], dtype="<i4").tobytes()).hexdigest() == ka["v_sha256"]
+
+
+def test_cli_state_checkpoint_save_and_resume(tmp_path, fixtures):
+    """-S 1 writes the final state and its t to <cnf>.assignment.txt; -L 1 resumes every
+    replica from it at that t (the reference's load_assignment, dynex.cc:2521-2532, values
+    read through a float).  The resumed CLI run equals the library resumed from the file."""
+    f = fixtures["n1000"]
+    form = dmm.from_arrays(f["lits"], f["off"], f["n"])
+    n, m = f["n"], f["m"]
+    path = str(tmp_path / "n1000.cnf")
+    dmm.write_cnf(form, path)
+    out = run_cli(["-i", path, "-l", "1", "-z", "40", "-S", "1"])
+    assert "s [0] UNKNOWN" in out
+    t_cap = float(re.search(r"STEPS = 40 \(T = ([0-9.]+)\)", out).group(1))
+    x_file, t_file = dmm.read_state(path + ".assignment.txt", n, m)
+    assert t_file == pytest.approx(t_cap, abs=1e-5)
+    # the library's own state after the same 40 steps, printed as the file holds it
+    x0, _ = dmm.initial_state_reference(form, 1, 0)
+    with dmm.Instance(form, precision="fp64") as inst:  # the CLI's default arithmetic
+        inst.set_state(x0)
+        inst.step(40)
+        x_lib, t_lib = inst.get_state()
+    assert np.array_equal(x_file, [float("%.15f" % v) for v in x_lib])
+    assert t_file == float("%.15f" % t_lib)
+    # resume: the CLI from the file against the library from the same (float-read) values
+    out2 = run_cli(["-i", path, "-l", "1", "-z", "25", "-L", "1"])
+    assert "LOADED, WILL START AT t=" in out2
+    steps2 = int(re.search(r"STEPS = (\d+)", out2).group(1))
+    t2 = float(re.search(r"STEPS = \d+ \(T = ([0-9.]+)\)", out2).group(1))
+    xr, tr = dmm.read_state(path + ".assignment.txt", n, m, reference_rounding=True)
+    with dmm.Instance(form, precision="fp64") as inst:
+        inst.set_state_at(xr, tr, 0)
+        r = inst.solve(max_steps=25)
+    assert steps2 == (r.solved_step if r.solved else r.steps)
+    assert t2 == pytest.approx(r.solved_t if r.solved else r.t, abs=1e-5)
+    assert t2 > tr
