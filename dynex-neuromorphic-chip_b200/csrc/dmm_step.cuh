@@ -87,6 +87,7 @@ struct TileSmem {
   StepAcc* acc;  // step accumulators (single-formula cooperative form), else null
   int ti;
   int flag;
+  int vnext;  // next 4-variable group of the sorted sums (reset by the tile loaders)
   double red[NT / 32];
   int cnt[2][NT / 32];
 };
@@ -109,6 +110,7 @@ __device__ __forceinline__ void load_tile(TileSmem<NT>& sm, const PackView<T>& P
       sm.snap.h = S->h_state;
       sm.cached = ii;
     }
+    sm.vnext = 0;
   }
   __syncthreads();
 }
@@ -309,13 +311,21 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
     // FP64 reference sums: four variables per warp, eight lanes each holding four entries
     // (entry e = lane-in-segment + 8 r); one bitonic network sorts the four lists at once
     // and the ascending left-to-right sum takes one shuffle per entry position for all four.
-    // Lists longer than 32 take the warp-wide sum afterwards.
+    // Lists longer than 32 take the warp-wide sum afterwards.  Warps take the groups from a
+    // shared counter: the long lists make groups uneven, and each variable's sum is
+    // computed by one warp alone, so the assignment does not change any result.
     static_assert(G == 32, "the sorted sum is organized per warp");
     constexpr int SEG = 8, NV = 32 / SEG, RR = 4;
     const double* ud = reinterpret_cast<const double*>(u);
     const double pinf = inf_val<double>();
     const int seg = lane / SEG, sl = lane % SEG;
-    for (int vb = sm.tile.begin + grp * NV; vb < v_end; vb += VPP * NV) {
+    (void)VPP;
+    (void)grp;
+    for (;;) {
+      int gi = 0;
+      if (lane == 0) gi = atomicAdd(&sm.vnext, 1);
+      const int vb = sm.tile.begin + NV * __shfl_sync(0xffffffffu, gi, 0);
+      if (vb >= v_end) break;
       const int v = vb + seg;
       const bool valid = v < v_end;
       int s0 = 0, d = 0;
@@ -616,6 +626,7 @@ __device__ __forceinline__ void load_tile_one(TileSmem<NT>& sm, const LocalSnap&
     sm.snap.set = ls.set;
     sm.snap.kcur = ls.kcur;
     sm.snap.h = ls.h;
+    sm.vnext = 0;
   }
   __syncthreads();
 }
