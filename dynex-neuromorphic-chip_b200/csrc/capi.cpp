@@ -114,7 +114,10 @@ dmm_status dmm_instance_create(const int32_t* lits, const int64_t* clause_off, i
   caps.clauses = m;
   caps.slots = clause_off[m];
   dmm_status st = inst->pack->init(caps, true, false);
-  if (st == DMM_OK) st = inst->pack->add(lits, clause_off, n, m, nullptr, nullptr, 0, &inst->idx);
+  // the literals are range-checked by the device CSR build (a host pass over a large
+  // formula costs milliseconds); commit_tiles reports a bad one
+  if (st == DMM_OK)
+    st = inst->pack->add(lits, clause_off, n, m, nullptr, nullptr, 0, &inst->idx, nullptr, true);
   if (st == DMM_OK) st = inst->pack->commit_tiles();
   if (st != DMM_OK) {
     delete inst;

@@ -343,9 +343,19 @@ __device__ __forceinline__ double sorted_sum(const double* u,
 // ---- setup, state I/O and the reference function-pair mirrors ---------------------------
 
 // Occurrence count of every variable (the reference's numOccurrenceT, dynex.cc:2380-2383).
-static __global__ void k_count(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ deg) {
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x)
-    atomicAdd(&deg[abs(lit[s]) - 1], 1);
+// Occurrence count per variable.  A literal 0 or outside [-n, n] is skipped and counted
+// in *bad (when given): formulas whose literals were not checked on the host are checked
+// here.
+static __global__ void k_count(const int32_t* __restrict__ lit, int nslots, int n,
+                               int32_t* __restrict__ deg, int32_t* bad) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
+    const int l = lit[s];
+    if (l == 0 || l > n || l < -n) {
+      if (bad) atomicAdd(bad, 1);
+      continue;
+    }
+    atomicAdd(&deg[abs(l) - 1], 1);
+  }
 }
 
 // Inclusive scan, 2048 elements per block; block totals to `sums`.
@@ -391,10 +401,12 @@ static __global__ void k_fill_start(const int32_t* __restrict__ vend, int n, int
     fill[v] = v > 0 ? vend[v - 1] : 0;
 }
 
-static __global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, int32_t* __restrict__ fill,
-                          int32_t* __restrict__ vslot) {
+static __global__ void k_scatter(const int32_t* __restrict__ lit, int nslots, int n,
+                                 int32_t* __restrict__ fill, int32_t* __restrict__ vslot) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
-    const int pos = atomicAdd(&fill[abs(lit[s]) - 1], 1);
+    const int l = lit[s];
+    if (l == 0 || l > n || l < -n) continue;  // counted by k_count
+    const int pos = atomicAdd(&fill[abs(l) - 1], 1);
     vslot[pos] = s;
   }
 }

@@ -55,8 +55,14 @@ struct DeviceScope {
 
 // Validates a formula given as flat literals + offsets.  Sets *k3 when every clause has
 // exactly three literals, and *may_have_units (if given) unless every clause has two or more.
+// check_literals = false skips the pass over the literals (the caller checks them on the
+// device, see Pack::add).
 dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n,
-                            int32_t m, bool* k3, bool* may_have_units = nullptr);
+                            int32_t m, bool* k3, bool* may_have_units = nullptr,
+                            bool check_literals = true);
+// First literal of lits[0, len) outside [-n, n] or zero: sets the error text and returns
+// DMM_ERR_LITERAL; DMM_OK when there is none.
+dmm_status locate_bad_literal(const int32_t* lits, int64_t len, int32_t n);
 // The checks of validate_formula that do not read the clauses or literals (shape of the
 // arrays and the slot count); the rest is checked when the formula is added to a pack.
 dmm_status validate_shape(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m);
@@ -100,9 +106,12 @@ class Pack {
 
   // x0 (n+2m doubles, optional): the instance starts runnable from this state, as after
   // set_state, with no read-back of its control record.
+  // device_literal_check: the literals are range-checked by the device CSR build instead of
+  // a host pass (large formulas); a bad literal is then reported by the next
+  // commit_tiles(), which the caller runs before using the formula.
   dmm_status add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
                  const dmm_params* p, const double* alpha_cm, int32_t max_steps, int32_t* idx,
-                 const double* x0 = nullptr);
+                 const double* x0 = nullptr, bool device_literal_check = false);
   dmm_status remove(int32_t idx);
   dmm_status set_params(int32_t idx, const dmm_params* p, const double* alpha_cm);
   dmm_status set_max_steps(int32_t idx, int32_t max_steps);

@@ -206,10 +206,10 @@ extern "C" dmm_status dmm_rhs3_f32_noalloc(const int32_t* lits, int32_t n, int32
     set_error("dmm_rhs3_f32_noalloc: %d literals outside [-n, n] or zero", nbad);
     return DMM_ERR_LITERAL;
   }
-  if (L > 0) k_count<<<grid, NA_THREADS, 0, st>>>(lits, L, s->vend);
+  if (L > 0) k_count<<<grid, NA_THREADS, 0, st>>>(lits, L, n, s->vend, nullptr);
   k_na_scan<<<1, NA_THREADS, 0, st>>>(s, n);
   k_fill_start<<<grid, NA_THREADS, 0, st>>>(s->vend, n, s->fill);
-  if (L > 0) k_scatter<<<grid, NA_THREADS, 0, st>>>(lits, L, s->fill, s->vslot);
+  if (L > 0) k_scatter<<<grid, NA_THREADS, 0, st>>>(lits, L, n, s->fill, s->vslot);
   k_sort_lists<<<grid, kThreads, (kThreads / 32) * kSortCap * sizeof(int32_t), st>>>(
       s->vend, n, s->vslot, s->longv, &s->counters[1], 0, NA_MAX_SLOTS / kSortCap + 2);
   DMM_CUDA(cudaGetLastError());

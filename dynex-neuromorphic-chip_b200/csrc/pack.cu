@@ -5,6 +5,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "dmm_inst.cuh"
 #include "dmm_step.cuh"
@@ -48,8 +50,49 @@ dmm_status validate_shape(const int32_t* lits, const int64_t* clause_off, int32_
   return DMM_OK;
 }
 
+// Runs f(lo, hi, t) over the chunks t of [0, len) on up to kValidateThreads host threads
+// when len is large (these passes are bound by memory bandwidth, which one core does not
+// reach); returns the number of chunks.  Falls back to one chunk on the calling thread
+// when no thread can be started.
+constexpr int kValidateThreads = 8;
+constexpr int64_t kValidateChunk = int64_t(1) << 18;  // elements per thread at least
+template <class F>
+static int host_parallel(int64_t len, F&& f) {
+  const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const int T = (int)std::max<int64_t>(
+      1, std::min<int64_t>({(int64_t)kValidateThreads, hw, len / kValidateChunk}));
+  if (T <= 1) {
+    f(int64_t(0), len, 0);
+    return 1;
+  }
+  const int64_t per = (len + T - 1) / T;
+  std::vector<std::thread> th;
+  try {
+    for (int t = 1; t < T; t++)
+      th.emplace_back([&f, t, per, len] { f(t * per, std::min(len, (t + 1) * per), t); });
+  } catch (...) {
+    for (auto& x : th) x.join();
+    f(int64_t(0), len, 0);
+    return 1;
+  }
+  f(int64_t(0), std::min(len, per), 0);
+  for (auto& x : th) x.join();
+  return T;
+}
+
+dmm_status locate_bad_literal(const int32_t* lits, int64_t len, int32_t n) {
+  for (int64_t s = 0; s < len; s++) {
+    const int32_t l = lits[s];
+    if (l == 0 || l > n || l < -n) {
+      set_error("formula: literal %d at position %lld out of range for n=%d", l, (long long)s, n);
+      return DMM_ERR_LITERAL;
+    }
+  }
+  return DMM_OK;
+}
+
 dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
-                            bool* k3, bool* may_have_units) {
+                            bool* k3, bool* may_have_units, bool check_literals) {
   if (n <= 0 || m < 0 || clause_off == nullptr) {
     set_error("formula: need n > 0, m >= 0 and clause offsets");
     return DMM_ERR_ARG;
@@ -58,12 +101,23 @@ dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int3
     set_error("formula: clause_off[0] must be 0");
     return DMM_ERR_ARG;
   }
-  // branch-free passes (they vectorize); the slow loops below only locate an error
+  // branch-free passes (they vectorize), split over host threads for large formulas; the
+  // slow loops below only locate an error
+  int64_t lmin_t[kValidateThreads], lmax_t[kValidateThreads];
+  const int nt_c = host_parallel(m, [&](int64_t lo, int64_t hi, int t) {
+    int64_t a = INT64_MAX, b = INT64_MIN;
+    for (int64_t c = lo; c < hi; c++) {
+      const int64_t len = clause_off[c + 1] - clause_off[c];
+      a = len < a ? len : a;
+      b = len > b ? len : b;
+    }
+    lmin_t[t] = a;
+    lmax_t[t] = b;
+  });
   int64_t lmin = INT64_MAX, lmax = INT64_MIN;
-  for (int32_t c = 0; c < m; c++) {
-    const int64_t len = clause_off[c + 1] - clause_off[c];
-    lmin = len < lmin ? len : lmin;
-    lmax = len > lmax ? len : lmax;
+  for (int t = 0; t < nt_c; t++) {
+    lmin = std::min(lmin, lmin_t[t]);
+    lmax = std::max(lmax, lmax_t[t]);
   }
   if (m > 0 && (lmin < 0 || lmax > DMM_MAX_CLAUSE_LITS)) {
     for (int32_t c = 0; c < m; c++) {
@@ -89,21 +143,18 @@ dmm_status validate_formula(const int32_t* lits, const int64_t* clause_off, int3
   }
   // -n <= l <= n, l != 0: (unsigned)l + n lies in [0, 2n]
   const uint32_t un = (uint32_t)n, span = 2u * (uint32_t)n;
-  uint32_t bad = 0;
-  for (int64_t s = 0; s < L; s++) {
-    const int32_t l = lits[s];
-    bad |= (uint32_t)(l == 0) | (uint32_t)((uint32_t)l + un > span);
-  }
-  if (bad) {
-    for (int64_t s = 0; s < L; s++) {
+  uint32_t bad_t[kValidateThreads];
+  const int nt_l = host_parallel(check_literals ? L : 0, [&](int64_t lo, int64_t hi, int t) {
+    uint32_t bad = 0;
+    for (int64_t s = lo; s < hi; s++) {
       const int32_t l = lits[s];
-      if (l == 0 || l > n || l < -n) {
-        set_error("formula: literal %d at position %lld out of range for n=%d", l, (long long)s,
-                  n);
-        return DMM_ERR_LITERAL;
-      }
+      bad |= (uint32_t)(l == 0) | (uint32_t)((uint32_t)l + un > span);
     }
-  }
+    bad_t[t] = bad;
+  });
+  uint32_t bad = 0;
+  for (int t = 0; t < nt_l; t++) bad |= bad_t[t];
+  if (bad) DMM_TRY(locate_bad_literal(lits, L, n));
   *k3 = m > 0 && lmin == 3 && lmax == 3;
   if (may_have_units) *may_have_units = m > 0 && lmin <= 1;
   return DMM_OK;
@@ -425,7 +476,7 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
   int32_t* vsl = vslot_ + I.slot0;
   DMM_CUDA(cudaMemsetAsync(vend, 0, (size_t)n * 4, stream_));
   if (L > 0) {
-    k_count<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, vend);
+    k_count<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, n, vend, ring_tail_d_ + 3);
     DMM_CUDA(cudaGetLastError());
   }
   const int64_t need = n / (kThreads * 8) + 64;
@@ -439,7 +490,7 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
   k_fill_start<<<blocks_for(n), kThreads, 0, stream_>>>(vend, n, fill);
   DMM_CUDA(cudaGetLastError());
   if (L > 0) {
-    k_scatter<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, fill, vsl);
+    k_scatter<<<blocks_for(L), kThreads, 0, stream_>>>(lit, L, n, fill, vsl);
     DMM_CUDA(cudaGetLastError());
   }
   // lists longer than the shared-memory sorter are appended to longv_d_ (count at
@@ -461,10 +512,24 @@ dmm_status Pack::build_csr(const InstDesc& I, const int32_t* lits_host) {
 
 dmm_status Pack::resolve_long_lists() {
   if (!long_pending_) return DMM_OK;
-  int32_t nlong = 0;
-  DMM_CUDA(cudaMemcpyAsync(&nlong, ring_tail_d_ + 2, sizeof(int32_t), cudaMemcpyDeviceToHost,
+  int32_t counts[2] = {0, 0};  // long lists, literals the CSR build found out of range
+  DMM_CUDA(cudaMemcpyAsync(counts, ring_tail_d_ + 2, sizeof counts, cudaMemcpyDeviceToHost,
                            stream_));
   DMM_CUDA(cudaStreamSynchronize(stream_));
+  const int32_t nlong = counts[0];
+  if (counts[1] > 0) {
+    // a formula admitted with device_literal_check holds a bad literal: name it as the host
+    // check would, then leave the counters for the caller to discard the pack
+    for (int32_t i = 0; i < (int32_t)live_.size(); i++) {
+      if (!live_[i]) continue;
+      const InstDesc& I = inst_h_[i];
+      std::vector<int32_t> h(I.nslots);
+      DMM_CUDA(cudaMemcpy(h.data(), lit_ + I.slot0, (size_t)I.nslots * 4, cudaMemcpyDeviceToHost));
+      DMM_TRY(locate_bad_literal(h.data(), I.nslots, I.n));
+    }
+    set_error("formula: %d literals out of range", counts[1]);
+    return DMM_ERR_LITERAL;
+  }
   if (nlong > 0) {
     // sorted on the host (setup only); an entry whose formula was removed meanwhile is
     // skipped, one whose range a later formula took is sorted again (harmless).  Past the
@@ -560,7 +625,7 @@ static dmm_status upload_alpha(T* dst, const double* a, int32_t m, cudaStream_t 
 
 dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, int32_t m,
                      const dmm_params* p, const double* alpha_cm, int32_t max_steps,
-                     int32_t* idx_out, const double* x0) {
+                     int32_t* idx_out, const double* x0, bool device_literal_check) {
   DMM_TRY(validate_shape(lits, clause_off, n, m));
   if (alpha_cm && !with_alpha_cm_) {
     set_error("this pack was created without per-clause alpha storage");
@@ -587,11 +652,12 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
     set_error("pack capacity exhausted (n=%d m=%d literals=%lld)", n, m, (long long)L);
     return DMM_ERR_BUDGET;
   }
-  // the literal upload runs while the host checks the clauses and literals
+  // the literal upload runs while the host checks the clauses (and literals)
   if (L > 0)
     DMM_CUDA(cudaMemcpyAsync(lit_ + slot0, lits, (size_t)L * 4, cudaMemcpyHostToDevice, stream_));
   bool k3 = false, units = true;
-  const dmm_status vst = validate_formula(lits, clause_off, n, m, &k3, &units);
+  const dmm_status vst =
+      validate_formula(lits, clause_off, n, m, &k3, &units, !device_literal_check);
   if (vst != DMM_OK) {
     cudaStreamSynchronize(stream_);
     var_alloc_.free(var0, n);
@@ -623,6 +689,7 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
     for (int32_t c = 0; c < m; c++)
       if (clause_off[c + 1] - clause_off[c] == 1) {
         const int32_t l = lits[clause_off[c]];
+        if (l == 0 || l > n || l < -n) continue;  // unchecked literal: the device check reports it
         unit_h_[std::abs(l) - 1] = l > 0 ? 1 : -1;
       }
     DMM_CUDA(cudaMemcpyAsync(unit_ + var0, unit_h_.data(), n, cudaMemcpyHostToDevice, stream_));

@@ -50,8 +50,14 @@ def test_instance_rejects_bad_formulas():
     def make(lits, off, n):
         return dmm.Formula(n, len(off) - 1, np.asarray(lits, np.int32),
                            np.asarray(off, np.int64), 1)
+    big, _ = dmm.generate_planted(100_000, 420_000, 0.08, 0.46, seed=5)
+    big_lits = big.lits.copy()
+    big_lits[1_000_001] = -100_001  # one bad literal deep inside a large formula
     cases = [(make([1, -2, 5], [0, 3], 3), "DMM_ERR_LITERAL"),
              (make([1, 0, 2], [0, 3], 3), "DMM_ERR_LITERAL"),
+             (make([7, 1, 2, 3], [0, 1, 4], 3), "DMM_ERR_LITERAL"),  # in a unit clause
+             (dmm.Formula(big.n, big.m, big_lits, big.clause_off, big.max_occurrence),
+              "DMM_ERR_LITERAL"),
              (make(list(range(1, 27)), [0, 26], 30), "DMM_ERR_CLAUSE_LEN"),
              (make([1, 2, 3], [0, 3, 2], 3), "DMM_ERR_ARG")]
     for form, name in cases:
@@ -59,6 +65,8 @@ def test_instance_rejects_bad_formulas():
             with pytest.raises(dmm.DmmError) as e:
                 dmm.Instance(form, precision=prec)
             assert e.value.name == name
+            if form.n == big.n:  # the literal checked on the device is named as on the host
+                assert "literal -100001 at position 1000001" in str(e.value)
     ok, _ = dmm.generate_planted(1_000, 4_200, 0.08, 0.46, seed=5)
     with dmm.Instance(ok, precision="fp32") as inst:
         inst.set_state(dmm.initial_state_uniform(ok, 6))
