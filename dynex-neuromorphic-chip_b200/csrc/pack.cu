@@ -414,6 +414,30 @@ void Pack::retire(void* p) {
 __global__ void k_put_desc(InstDesc* dst, InstDesc d) { *dst = d; }
 __global__ void k_put_ctrl(InstCtrl* dst, InstCtrl c) { *dst = c; }
 
+// Signs of V on the device (the control record says which candidate holds it), so that
+// one byte per variable crosses to the host: pre from the solving step's V (0 for V == 0;
+// flag[0] = 1 when the formula is not solved), post from the current V (+1 / -1).
+template <class T>
+__global__ void k_signs(const InstCtrl* __restrict__ ctrl, const T* __restrict__ cand,
+                        int64_t var_cap, int64_t var0, int n, int8_t* pre, int8_t* post,
+                        int32_t* flag) {
+  const InstCtrl c = *ctrl;
+  if (pre && c.solved_step < 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *flag = 1;
+    pre = nullptr;
+  }
+  const T* vs = cand + (int64_t)(c.sol_set * kTrials + c.sol_k) * var_cap + var0;
+  const T* vc = cand + (int64_t)(c.set * kTrials + c.kcur) * var_cap + var0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (pre) {
+      const T v = vs[i];
+      pre[i] = v > T(0) ? 1 : (v < T(0) ? -1 : 0);
+    }
+    if (post) post[i] = vc[i] > T(0) ? 1 : -1;
+  }
+}
+
+
 dmm_status Pack::upload_desc(int32_t idx) {
   k_put_desc<<<1, 1, 0, stream_>>>(inst_d_ + idx, inst_h_[idx]);
   DMM_CUDA(cudaGetLastError());
@@ -1409,9 +1433,11 @@ dmm_status Pack::preload_kernels() {
   if (prec_ == DMM_FP64) {
     fns.push_back((const void*)k_set_state<double>);
     fns.push_back((const void*)k_get_state<double>);
+    fns.push_back((const void*)k_signs<double>);
   } else {
     fns.push_back((const void*)k_set_state<float>);
     fns.push_back((const void*)k_get_state<float>);
+    fns.push_back((const void*)k_signs<float>);
     fns.push_back(persist_fn_x<true>(prec_, G));
     fns.push_back(staged_fn(G));
     fns.push_back((const void*)k_xp_count<kXprepThreads>);
@@ -1709,40 +1735,33 @@ dmm_status Pack::dostep(int32_t idx, const double* x, const double* dxdt, double
   return DMM_OK;
 }
 
-template <class T>
-static dmm_status signs_of(const T* dV, int32_t n, int8_t* out, bool zero_as_zero, cudaStream_t s) {
-  std::vector<T> h(n);
-  DMM_CUDA(cudaMemcpyAsync(h.data(), dV, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, s));
-  DMM_CUDA(cudaStreamSynchronize(s));
-  for (int32_t i = 0; i < n; i++)
-    out[i] = h[i] > T(0) ? 1 : ((h[i] < T(0) || !zero_as_zero) ? -1 : 0);
-  return DMM_OK;
-}
-
 dmm_status Pack::assignment(int32_t idx, int8_t* pre, int8_t* post) {
   if (!live(idx)) return DMM_ERR_ARG;
-  InstCtrl c;
-  DMM_TRY(read_ctrl(idx, &c));
+  if (!pre && !post) return DMM_OK;
   const InstDesc& I = inst_h_[idx];
-  auto vptr = [&](int set, int k) -> const void* {
-    return static_cast<const char*>(cand_) +
-           ((int64_t)(set * kTrials + k) * caps_.vars + I.var0) * (int64_t)tsize_;
-  };
-  if (pre) {
-    if (c.solved_step < 0) {
-      set_error("instance %d is not solved", idx);
-      return DMM_ERR_STATE;
-    }
-    if (prec_ == DMM_FP64)
-      DMM_TRY(signs_of(static_cast<const double*>(vptr(c.sol_set, c.sol_k)), I.n, pre, true, stream_));
-    else
-      DMM_TRY(signs_of(static_cast<const float*>(vptr(c.sol_set, c.sol_k)), I.n, pre, true, stream_));
-  }
-  if (post) {
-    if (prec_ == DMM_FP64)
-      DMM_TRY(signs_of(static_cast<const double*>(vptr(c.set, c.kcur)), I.n, post, false, stream_));
-    else
-      DMM_TRY(signs_of(static_cast<const float*>(vptr(c.set, c.kcur)), I.n, post, false, stream_));
+  // [flag | pre (n) | post (n)] in the staging buffer
+  DMM_TRY(ensure_stage(1 + (2 * (int64_t)I.n + 7) / 8));
+  int32_t* flag = reinterpret_cast<int32_t*>(stage_);
+  int8_t* dpre = reinterpret_cast<int8_t*>(stage_) + 8;
+  int8_t* dpost = dpre + I.n;
+  DMM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int32_t), stream_));
+  if (prec_ == DMM_FP64)
+    k_signs<double><<<blocks_for(I.n), kThreads, 0, stream_>>>(
+        ctrl_d_ + idx, static_cast<const double*>(cand_), caps_.vars, I.var0, I.n,
+        pre ? dpre : nullptr, post ? dpost : nullptr, flag);
+  else
+    k_signs<float><<<blocks_for(I.n), kThreads, 0, stream_>>>(
+        ctrl_d_ + idx, static_cast<const float*>(cand_), caps_.vars, I.var0, I.n,
+        pre ? dpre : nullptr, post ? dpost : nullptr, flag);
+  DMM_CUDA(cudaGetLastError());
+  int32_t not_solved = 0;
+  DMM_CUDA(cudaMemcpyAsync(&not_solved, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+  if (pre) DMM_CUDA(cudaMemcpyAsync(pre, dpre, I.n, cudaMemcpyDeviceToHost, stream_));
+  if (post) DMM_CUDA(cudaMemcpyAsync(post, dpost, I.n, cudaMemcpyDeviceToHost, stream_));
+  DMM_CUDA(cudaStreamSynchronize(stream_));
+  if (pre && not_solved) {
+    set_error("instance %d is not solved", idx);
+    return DMM_ERR_STATE;
   }
   return DMM_OK;
 }
