@@ -679,6 +679,16 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
   // the literal upload runs while the host checks the clauses (and literals)
   if (L > 0)
     DMM_CUDA(cudaMemcpyAsync(lit_ + slot0, lits, (size_t)L * 4, cudaMemcpyHostToDevice, stream_));
+  InstDesc I{};
+  I.n = n;
+  I.m = m;
+  I.var0 = var0;
+  I.cls0 = cls0;
+  I.slot0 = slot0;
+  I.nslots = (int32_t)L;
+  // with the literals checked on the device the occurrence lists need nothing from the
+  // host pass: they build while the host checks the clause offsets
+  if (device_literal_check) DMM_TRY(build_csr(I, lits));
   bool k3 = false, units = true;
   const dmm_status vst =
       validate_formula(lits, clause_off, n, m, &k3, &units, !device_literal_check);
@@ -689,13 +699,6 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
     slot_alloc_.free(slot0, L);
     return vst;
   }
-  InstDesc I{};
-  I.n = n;
-  I.m = m;
-  I.var0 = var0;
-  I.cls0 = cls0;
-  I.slot0 = slot0;
-  I.nslots = (int32_t)L;
   I.k3 = k3 ? 1 : 0;
   I.has_alpha_cm = alpha_cm ? 1 : 0;
   I.max_steps = max_steps;
@@ -726,7 +729,7 @@ dmm_status Pack::add(const int32_t* lits, const int64_t* clause_off, int32_t n, 
     else
       DMM_TRY(upload_alpha(static_cast<float*>(alpha_cm_) + cls0, alpha_cm, m, stream_));
   }
-  DMM_TRY(build_csr(I, lits));
+  if (!device_literal_check) DMM_TRY(build_csr(I, lits));
   inst_h_[idx] = I;
   live_[idx] = 1;
   add_serial_[idx] = ++add_counter_;
