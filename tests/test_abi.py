@@ -166,3 +166,22 @@ def test_state_checkpoint_file_format(tmp_path):
     with pytest.raises(dmm.DmmError) as e:
         dmm.read_state(str(tmp_path / "missing.txt"), n, m)
     assert e.value.name == "DMM_ERR_IO"
+
+
+def test_validation_of_large_formulas_split_over_threads():
+    """The host checks of large formulas run on several threads; an error anywhere, in the
+    last chunk too, is still found and named."""
+    f, _ = dmm.generate_planted(200_000, 800_000, 0.08, 0.46, seed=9)
+    assert dmm.from_arrays(f.lits, f.clause_off, f.n).m == f.m
+    for pos in (5, len(f.lits) // 2 + 1, len(f.lits) - 1):
+        bad = f.lits.copy()
+        bad[pos] = f.n + 1
+        with pytest.raises(dmm.DmmError) as e:
+            dmm.from_arrays(bad, f.clause_off, f.n)
+        assert e.value.name == "DMM_ERR_LITERAL"
+        assert f"literal {f.n + 1} at position {pos}" in str(e.value)
+    off = f.clause_off.copy()
+    off[-2] = off[-3] - 1  # offsets decrease near the end
+    with pytest.raises(dmm.DmmError) as e:
+        dmm.from_arrays(f.lits, off, f.n)
+    assert e.value.name == "DMM_ERR_ARG"
