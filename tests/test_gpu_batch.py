@@ -141,6 +141,21 @@ def test_full_size_fp32_bitexact_vs_oracle_first_steps(big):
             assert np.array_equal(inst.get_state()[0], ref["dump"][r])
 
 
+def test_full_size_fp64_bitexact_vs_oracle_first_steps(big):
+    """n = 100,000, m = 800,000 in the reference's FP64 arithmetic (sorted per-variable sums,
+    warps taking variable groups dynamically): the first 6 steps equal the oracle's."""
+    form, _ = big
+    x0 = dmm.initial_state_uniform(form, 79)
+    o = Oracle(form.n, form.m, form.lits, form.clause_off, precision="fp64")
+    ref = o.run(x0, 6, dump_every=3)
+    with dmm.Instance(form, precision="fp64") as inst:
+        assert inst.launch_form == "cooperative"
+        inst.set_state(x0)
+        for r in range(1, 3):
+            inst.step(3)
+            assert np.array_equal(inst.get_state()[0], ref["dump"][r])
+
+
 def test_full_size_fp32_properties(big):
     """Determinism, state bounds and the unsatisfied count against a host recount."""
     form, planted = big
