@@ -35,6 +35,7 @@ constexpr uint16_t kXpPad = 0xFFFF;  // xdst of a padding entry
 constexpr int kArriveBits = 12;      // width of one trial's arrival count (> grid size)
 constexpr int kPollSleepNs = 64;     // back-off between polls of a barrier word
 
+
 __host__ __device__ constexpr int xp_align16(int bytes) { return (bytes + 15) & ~15; }
 
 // Dynamic shared-memory layout of the staged form (byte offsets).
@@ -249,24 +250,62 @@ __global__ void __launch_bounds__(NT, 1)
         *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
         *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
       };
-      for (int g = g0; g < c_end; g += 4 * NT) {
-        if (g + 4 <= c_end) {
-          Group4 q;
-          load_words4(q, ll, sp, g);
-          load_state4(q, Xs, Xl, Cp, acm, kc.alpha, pending, g);
-          group(q, g);
-        } else {
-          for (int c = g; c < c_end; c++) {
-            T xs = Xs[c], xl = Xl[c];
-            const T cp = pending ? Cp[c] : T(0);
-            const T al = acm ? acm[c] : kc.alpha;
-            Cp[c] = one(__ldg(ll + 3 * c), __ldg(ll + 3 * c + 1), __ldg(ll + 3 * c + 2),
-                        __ldg(sp + 3 * c), __ldg(sp + 3 * c + 1), __ldg(sp + 3 * c + 2), xs, xl,
-                        cp, al);
-            Xs[c] = xs;
-            Xl[c] = xl;
+      auto single = [&](int c) {
+        T xs = Xs[c], xl = Xl[c];
+        const T cp = pending ? Cp[c] : T(0);
+        const T al = acm ? acm[c] : kc.alpha;
+        Cp[c] = one(__ldg(ll + 3 * c), __ldg(ll + 3 * c + 1), __ldg(ll + 3 * c + 2),
+                    __ldg(sp + 3 * c), __ldg(sp + 3 * c + 1), __ldg(sp + 3 * c + 2), xs, xl, cp,
+                    al);
+        Xs[c] = xs;
+        Xl[c] = xl;
+      };
+      // rounds of 4-clause groups (one per thread); a remainder of at most 2 NT clauses
+      // goes out as pairs, so that the last round spreads over twice as many threads with
+      // half the work each
+      const int count = c_end - c_begin;
+      const int full_end = c_begin + count / (4 * NT) * (4 * NT);
+      const int rem = c_end - full_end;
+      const bool pairs = rem <= 2 * NT;
+      const int g_end = pairs ? full_end : full_end + (rem & ~3);
+      for (int g = g0; g < g_end; g += 4 * NT) {
+        Group4 q;
+        load_words4(q, ll, sp, g);
+        load_state4(q, Xs, Xl, Cp, acm, kc.alpha, pending, g);
+        group(q, g);
+      }
+      if (pairs) {
+        const int c = full_end + 2 * tid;  // even: 4-byte aligned words, 8-byte state
+        if (c + 2 <= c_end) {
+          const int* L3 = reinterpret_cast<const int*>(ll + 3 * c);
+          const unsigned* Q3 = reinterpret_cast<const unsigned*>(sp + 3 * c);
+          int lw[3];
+          unsigned qw[3];
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            lw[r] = __ldg(L3 + r);
+            qw[r] = __ldg(Q3 + r);
           }
+          auto lit = [&](int k) {
+            return (k & 1) ? (lw[k >> 1] >> 16) : (int)(short)(lw[k >> 1] & 0xffff);
+          };
+          auto pos = [&](int k) { return (int)((k & 1) ? (qw[k >> 1] >> 16) : (qw[k >> 1] & 0xffffu)); };
+          const float2 xs2 = *reinterpret_cast<const float2*>(Xs + c);
+          const float2 xl2 = *reinterpret_cast<const float2*>(Xl + c);
+          const float2 cp2 = pending ? *reinterpret_cast<const float2*>(Cp + c) : make_float2(0.f, 0.f);
+          const float2 al2 = acm ? *reinterpret_cast<const float2*>(acm + c)
+                                 : make_float2(kc.alpha, kc.alpha);
+          T xs[2] = {xs2.x, xs2.y}, xl[2] = {xl2.x, xl2.y}, cc[2];
+          cc[0] = one(lit(0), lit(1), lit(2), pos(0), pos(1), pos(2), xs[0], xl[0], cp2.x, al2.x);
+          cc[1] = one(lit(3), lit(4), lit(5), pos(3), pos(4), pos(5), xs[1], xl[1], cp2.y, al2.y);
+          *reinterpret_cast<float2*>(Xs + c) = make_float2(xs[0], xs[1]);
+          *reinterpret_cast<float2*>(Xl + c) = make_float2(xl[0], xl[1]);
+          *reinterpret_cast<float2*>(Cp + c) = make_float2(cc[0], cc[1]);
+        } else if (c < c_end) {
+          single(c);
         }
+      } else if (g_end + tid < c_end) {
+        single(g_end + tid);  // fewer than 4 clauses
       }
       unsat = warp_sum_i(unsat);
       vfail = warp_sum_i(vfail);
