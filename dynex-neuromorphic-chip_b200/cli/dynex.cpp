@@ -4,6 +4,7 @@
 //   dynex -i file.cnf [-l seed] [-w replicas] [-u walltime] [-z maxsteps]
 //         [-c alpha] [-b beta] [-n gamma] [-h delta] [-j epsilon] [-k zeta] [-m xl_max]
 //         [-q 0|1] [-p 0|1] [-P fp64|fp32] [-D device] [-L 0|1] [-S 0|1]
+//         [-t 1 [-s iterations] [-v switchfraction] [-g 0|1|2] [-x err1] [-y err2] [-d init_dt]]
 //
 // Defaults follow the reference (FP64 arithmetic, seed 0, one replica); with them the
 // reported step count, T and assignment equal the reference's.  -P fp32 selects the
@@ -15,16 +16,19 @@
 // ask for anything but the default.  -S 1 writes the final state of the reported replica
 // to <cnf>.assignment.txt in the reference's checkpoint format (dynex.cc:2131-2135); -L 1
 // starts every replica from that file, at its time t, as the reference's load_assignment
-// does (dynex.cc:2521-2532, 2688-2692; a compile-time switch there).
+// does (dynex.cc:2521-2532, 2688-2692; a compile-time switch there).  -t 1 runs the
+// reference's simulated-annealing parameter tuner with the replicas as its chains.
 #include <getopt.h>
 #include <unistd.h>
 
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -117,7 +121,9 @@ void usage(const char* argv0) {
       "c   -P fp64|fp32  arithmetic (default fp64, the reference's)\n"
       "c   -D int      CUDA device\n"
       "c   -L 0|1      start from <file>.assignment.txt (V, Xs, Xl and t)\n"
-      "c   -S 0|1      write the final state to <file>.assignment.txt\n");
+      "c   -S 0|1      write the final state to <file>.assignment.txt\n"
+      "c   -t 1        tune the parameters (simulated annealing, one chain per replica):\n"
+      "c               -s iterations, -v switchfraction, -g 0|1|2 params, -z steps per run\n");
 }
 
 bool fail(dmm_status st, const char* what) {
@@ -130,11 +136,247 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// ---- parameter tuner (-t 1) ---------------------------------------------------------------
+// The reference's simulated-annealing tuner (dynex.cc:1575-2201) in its default form
+// (tune_mode 0: every iteration starts the replicas from their original states, perturbed by
+// `switchfraction`).  Replicas are Metropolis chains over the nine parameters (alpha .. zeta,
+// the two Runge-Kutta tolerances and init_dt; the default integrator uses the first six);
+// a chain's objective is the lowest loc its replica reaches in a run (dynex.cc:537, 640).
+// Proposals, acceptance and the random-number use follow the reference step by step (one
+// std::mt19937 seeded with -l, the same distributions drawn in the same order), so the
+// parameter sequence depends only on the objectives.  Each iteration runs all replicas as one
+// batch on the GPU, each to the step cap (-z) or its solution; the reference's threads also
+// stop when any of them solves, a race this build does not reproduce.  The initial objective
+// is the loc of each replica's initial state (the reference takes one Euler step through
+// odeint, dynex.cc:1711-1716, whose one right-hand side sees that state).
+struct TuneOpts {
+  int iterations = INT_MAX;       // -s
+  double switchfraction = 0.0001; // -v
+  int params = 2;                 // -g: 0 alpha..zeta, 1 the integrator's, 2 all
+  double err1 = 0.52, err2 = 0.10, init_dt = 0.15;  // -x -y -d (dynex.cc:151-153)
+};
+
+constexpr int kParams = 9;
+enum { kLBH = 0, kHBH = 1, kLBS = 2, kHBS = 3 };  // dynex.cc:72-75
+
+int run_tuner(const Opts& o, const TuneOpts& to, const dmm_cnf* cnf) {
+  const int n = cnf->n, m = cnf->m, R = o.replicas;
+  const int64_t N = (int64_t)n + 2 * (int64_t)m;
+  // default (large) bounds, dynex.cc:1607-1634: {hard low, hard high, soft low, soft high}
+  const double bounds[kParams][4] = {
+      {1e-15, 100.0, 0.01, 1.0},  {1e-15, 100.0, 0.01, 1.0},  {1e-15, 0.5, 0.01, 0.25},
+      {1e-15, 1.0, 0.01, 0.25},   {1e-15, 0.5, 0.01, 0.25},   {1e-15, 1.0, 0.01, 0.25},
+      {1e-15, 1.0, 0.01, 1.0},    {1e-15, 1.0, 0.01, 1.0},    {1e-15, 1.0, 1e-15, 0.00001}};
+  std::vector<double> par((size_t)R * kParams), rem_par((size_t)R * kParams);
+  std::vector<double> rem_x((size_t)R * N), x0((size_t)R * N);
+  for (int i = 0; i < R; i++) {
+    int32_t div = 1;
+    if (fail(dmm_initial_state_reference(cnf->lits, cnf->clause_off, n, m, o.seed, i,
+                                         rem_x.data() + (size_t)i * N, &div), "initial state"))
+      return EXIT_FAILURE;
+    const double p[kParams] = {o.p.alpha / div, o.p.beta, o.p.gamma, o.p.delta, o.p.epsilon,
+                               o.p.zeta, to.err1, to.err2, to.init_dt};
+    std::copy(p, p + kParams, par.begin() + (size_t)i * kParams);
+  }
+  std::mt19937 gen(o.seed);  // dynex.cc:1684
+  int p_low = 0, p_high = kParams - 1;
+  if (to.params == 0) p_high = 5;
+  if (to.params == 1) p_low = 6;
+  std::uniform_int_distribution<int> rand_param(p_low, p_high);
+  std::uniform_real_distribution<double> rand_r(0.0, 1.0);
+  std::uniform_int_distribution<int> rand_switch(0, n - 1);
+  std::uniform_int_distribution<int> rand_v(-1, 1);
+  std::uniform_int_distribution<int> rand_mode(0, 2);
+  std::vector<double> best(R), curr(R), cand(R), ssf(R, 100.0);
+  std::vector<int> no_impr(R, 0), nchange(R, 0), best_loc(R, m), loc_zero(R, 0);
+  std::vector<int> tune_p((size_t)R * kParams, -1), rem_tune_p((size_t)R * kParams, -1);
+  // one batch run of every replica from x0 with its parameters: lowest loc of each
+  auto evaluate = [&](int max_steps, double wall) -> bool {
+    dmm_batch* b = nullptr;
+    if (fail(dmm_batch_create(o.prec, o.device, R, (int64_t)n * R, (int64_t)m * R,
+                              cnf->nlits * R, &b), "creating the batch"))
+      return false;
+    bool ok = true;
+    for (int i = 0; i < R && ok; i++) {
+      dmm_params p = o.p;
+      const double* q = par.data() + (size_t)i * kParams;
+      p.alpha = q[0]; p.beta = q[1]; p.gamma = q[2]; p.delta = q[3]; p.epsilon = q[4]; p.zeta = q[5];
+      int32_t idx = 0;
+      ok = !fail(dmm_batch_add(b, cnf->lits, cnf->clause_off, n, m, &p, x0.data() + (size_t)i * N,
+                               max_steps, &idx), "adding a replica");
+    }
+    dmm_batch_stats st{};
+    ok = ok && !fail(dmm_batch_run(b, wall, &st), "integration");
+    for (int i = 0; i < R && ok; i++) {
+      dmm_report rep{};
+      ok = !fail(dmm_batch_result(b, i, &rep, nullptr), "result");
+      best_loc[i] = rep.best_loc;
+      loc_zero[i] = rep.status == DMM_SOLVED;
+    }
+    dmm_batch_destroy(b);
+    return ok;
+  };
+  const bool q = o.quiet;
+  if (!q) {
+    std::printf("c [TUNE] MODE           : 0\n");
+    std::printf("c [TUNE] N_ITERATIONS   : %d\n", to.iterations);
+    std::printf("c [TUNE] SWITCHFRACTION : %.15f\n", to.switchfraction);
+    std::printf("c [TUNE] INITIAL OBJECTIVE...\n");
+  }
+  // initial objective: loc of each replica's initial state (energy = loc when tuning)
+  {
+    dmm_instance* inst = nullptr;
+    if (fail(dmm_instance_create(cnf->lits, cnf->clause_off, n, m, o.prec, o.device, &inst),
+             "creating the instance"))
+      return EXIT_FAILURE;
+    std::vector<double> dx(N);
+    for (int i = 0; i < R; i++) {
+      int32_t loc = 0;
+      double e = 0.0;
+      if (fail(dmm_instance_rhs(inst, rem_x.data() + (size_t)i * N, dx.data(), &loc, &e), "rhs")) {
+        dmm_instance_destroy(inst);
+        return EXIT_FAILURE;
+      }
+      best[i] = curr[i] = std::min(loc, m);
+    }
+    dmm_instance_destroy(inst);
+  }
+  const std::string tuning_file = o.input + ".tuning.txt";
+  if (FILE* f = std::fopen(tuning_file.c_str(), "w")) {  // dynex.cc:2719-2726
+    std::fprintf(f, "ITERATION;INSTANCE;PARAM_01;PARAM_02;PARAM_03;PARAM_04;PARAM_05;PARAM_06;"
+                    "PARAM_07;ENERGY\n");
+    std::fclose(f);
+  }
+  double tune_global = m;
+  int max_steps = o.max_steps;
+  double wall = o.walltime;
+  bool change_params = false, solved = false;
+  int switch_count = 0;
+  for (int iter = 0; iter < to.iterations && !solved; iter++) {
+    std::printf("c [TUNE] ITERATION %d. GLOBAL=%g\n", iter, tune_global);
+    int min_no_impr = INT_MAX;
+    for (int i = 0; i < R; i++) {
+      min_no_impr = std::min(min_no_impr, no_impr[i]);
+      std::copy(par.begin() + (size_t)i * kParams, par.begin() + (size_t)(i + 1) * kParams,
+                rem_par.begin() + (size_t)i * kParams);
+      double* xi = x0.data() + (size_t)i * N;
+      std::copy(rem_x.begin() + (size_t)i * N, rem_x.begin() + (size_t)(i + 1) * N, xi);
+      if (iter > 0) {  // switchfraction (dynex.cc:1858-1866)
+        switch_count = (int)std::abs(n * to.switchfraction);
+        if (to.switchfraction > 0 && switch_count == 0) switch_count = 1;
+        for (int j = 0; j < switch_count; j++) {
+          const int v = rand_switch(gen);
+          xi[v] = rand_v(gen);
+        }
+      }
+    }
+    if (min_no_impr >= 25) {  // dynex.cc:1870-1917 (tune_mode 0 part)
+      wall *= 2;
+      max_steps = max_steps > 0 ? (int)std::min<int64_t>(2 * (int64_t)max_steps, INT_MAX) : 0;
+      if (!q) std::printf("c [TUNE] NOTHING IMPROVED SINCE 25 ITERATIONS. maxsteps TO %d\n", max_steps);
+      std::fill(no_impr.begin(), no_impr.end(), 0);
+      std::fill(ssf.begin(), ssf.end(), 100.0);
+      change_params = false;
+    }
+    for (int i = 0; i < R; i++) {
+      nchange[i] = 0;
+      for (int k = 0; k < kParams; k++) rem_tune_p[(size_t)i * kParams + k] = -1;
+    }
+    if (change_params) {
+      for (int i = 0; i < R; i++) {
+        double* pi = par.data() + (size_t)i * kParams;
+        if (no_impr[i] > 0 && no_impr[i] % 10 == 0) ssf[i] = std::min(ssf[i] * 10, 1e12);
+        const int mode = rand_mode(gen);
+        std::lognormal_distribution<double> rand_num(0.0, 0.5);
+        int nc = (int)rand_num(gen);
+        nc = std::max(1, std::min(nc, kParams));
+        nchange[i] = nc;
+        for (int k = 0; k < nc; k++) {
+          int& tp = tune_p[(size_t)i * kParams + k];
+          int& rtp = rem_tune_p[(size_t)i * kParams + k];
+          tp = rtp == -1 ? rand_param(gen) : rtp;
+          rtp = tp;
+          const double* bd = bounds[tp];
+          double c = pi[tp];
+          if (mode == 0) {  // small move (dynex.cc:1972-1995)
+            const double soft = bd[kHBS] - bd[kLBS];
+            std::uniform_real_distribution<double> rand_p(0, soft);
+            (void)rand_p(gen);  // drawn and overwritten in the reference
+            std::uniform_real_distribution<double> rand_move(-1.5, 1.5);
+            const double move = rand_move(gen);
+            c = pi[tp] + pi[tp] * move / ssf[i];
+            if (c <= 0.0) c = 1e-8;
+          } else {  // a point within the soft (1) or hard (2) bounds (dynex.cc:1998-2058)
+            const double lo = mode == 1 ? bd[kLBS] : bd[kLBH];
+            const double hi = mode == 1 ? bd[kHBS] : bd[kHBH];
+            std::uniform_real_distribution<double> rand_b(lo, hi);
+            c = rand_b(gen);
+            if (tp == 4 && c >= pi[2]) c = pi[2] - 0.1;
+          }
+          pi[tp] = c;
+        }
+        if (!q) {
+          std::printf("c [TUNE] [%d] -c=%.15f -b=%.15f -n=%.15f -h=%.15f -j=%.15f -k=%.15f "
+                      "-x=%.15f -y=%.15f -d=%.15f\n", i, pi[0], pi[1], pi[2], pi[3], pi[4], pi[5],
+                      pi[6], pi[7], pi[8]);
+        }
+      }
+    }
+    change_params = true;
+    if (!evaluate(max_steps, wall > 0 ? wall : 0.0)) return EXIT_FAILURE;
+    for (int i = 0; i < R; i++) {
+      cand[i] = best_loc[i];
+      if (cand[i] < tune_global) {
+        tune_global = cand[i];
+        const double* pi = par.data() + (size_t)i * kParams;
+        if (FILE* f = std::fopen(tuning_file.c_str(), "a")) {  // dynex.cc:2127-2129
+          std::fprintf(f, "%d;%d;%.15f;%.15f;%.15f;%.15f;%.15f;%.15f;%.15f;%.15f\n", iter, i,
+                       pi[0], pi[1], pi[2], pi[3], pi[4], pi[5], pi[8], tune_global);
+          std::fclose(f);
+        }
+        if (!q) std::printf("c [TUNE] [%d] NEW GLOBAL %g\n", i, tune_global);
+      }
+    }
+    for (int i = 0; i < R; i++) {  // Metropolis (dynex.cc:2149-2184)
+      if (cand[i] < best[i]) {
+        best[i] = cand[i];
+        if (loc_zero[i] || best_loc[i] == 0) {
+          solved = true;
+          break;
+        }
+      }
+      const double diff = cand[i] - curr[i] + 1.0;
+      const double temp = 1.0 / double(iter + 1);
+      const double metropolis = std::exp(-diff / temp);
+      if (diff < 0 || rand_r(gen) < metropolis) {
+        std::printf("c [TUNE] [%d] %d CANDIDATES ACCEPTED (E=%g, temp=%g)\n", i, nchange[i], cand[i],
+                    temp);
+        curr[i] = cand[i];
+        no_impr[i] = 0;
+      } else {
+        for (int k = 0; k < nchange[i]; k++) {
+          const int tp = tune_p[(size_t)i * kParams + k];
+          par[(size_t)i * kParams + tp] = rem_par[(size_t)i * kParams + tp];
+          rem_tune_p[(size_t)i * kParams + k] = -1;
+        }
+        std::printf("c [TUNE] [%d] CANDIDATE REJECTED (E=%g, temp=%g)\n", i, cand[i], temp);
+        no_impr[i]++;
+      }
+    }
+  }
+  std::printf(solved ? "c [TUNE] SOLUTION FOUND.\nc [TUNE] FINISHED.\n" : "c [TUNE] FINISHED.\n");
+  std::printf("%g", tune_global);
+  std::fflush(stdout);
+  return EXIT_SUCCESS;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   Opts o;
   dmm_params_default(&o.p);
+  TuneOpts to;
+  bool tune = false;
   int c;
   while ((c = getopt(argc, argv, "i:l:w:u:z:c:b:n:h:j:k:m:q:P:D:L:S:o:t:p:e:f:g:r:v:x:y:d:a:s:")) != -1) {
     const char* a = optarg;
@@ -160,9 +402,13 @@ int main(int argc, char** argv) {
       case 'o':
         if (std::atoi(a) != 6) std::fprintf(stderr, "c -o %s: only the default integrator (6) is available\n", a);
         break;
-      case 't':
-        if (std::atoi(a) != 0) std::fprintf(stderr, "c -t %s: tuning mode is not available\n", a);
-        break;
+      case 't': tune = std::atoi(a) != 0; break;
+      case 's': to.iterations = (int)std::atof(a); break;
+      case 'v': to.switchfraction = std::atof(a); break;
+      case 'g': to.params = std::atoi(a); break;
+      case 'x': to.err1 = std::atof(a); break;
+      case 'y': to.err2 = std::atof(a); break;
+      case 'd': to.init_dt = std::atof(a); break;
       case 'p': o.heuristics = std::atoi(a) != 0; break;
       default:
         break;  // other reference options only affect modes outside the default path
@@ -195,6 +441,12 @@ int main(int argc, char** argv) {
     std::printf("c ALPHA %.15f BETA %.15f GAMMA %.15f DELTA %.15f EPSILON %.15f ZETA %.15f\n",
                 o.p.alpha, o.p.beta, o.p.gamma, o.p.delta, o.p.epsilon, o.p.zeta);
     std::printf("c SEED      : %d\n", o.seed);
+  }
+  if (tune) {
+    if (!o.quiet) std::printf("c [TUNE] TUNING CIRCUIT...\n");
+    const int rc = run_tuner(o, to, cnf);
+    dmm_cnf_free(cnf);
+    return rc;
   }
   const int64_t N = (int64_t)n + 2 * (int64_t)m;
   std::vector<double> x(N);

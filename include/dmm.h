@@ -152,7 +152,7 @@ dmm_status dmm_cnf_from_arrays(const int32_t* lits, const int64_t* clause_off, i
                                int32_t m, dmm_cnf** out);
 void dmm_cnf_free(dmm_cnf* cnf);
 /* Writes DIMACS; planted (n signs, may be NULL) is written as a `c [ ... ]` first line
- * like the reference fixtures (cnf/*.cnf line 1). */
+ * like the first line of the reference's fixture files. */
 dmm_status dmm_cnf_write(const dmm_cnf* cnf, const char* path, const int8_t* planted);
 /* Planted random k=3 SAT: a planted assignment is drawn from `seed`; each clause has 3
  * distinct variables; literal signs are drawn so that the number of literals agreeing with

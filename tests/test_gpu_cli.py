@@ -136,3 +136,50 @@ def test_cli_state_checkpoint_save_and_resume(tmp_path, fixtures):
     assert steps2 == (r.solved_step if r.solved else r.steps)
     assert t2 == pytest.approx(r.solved_t if r.solved else r.t, abs=1e-5)
     assert t2 > tr
+
+
+def _tune(path, *args):
+    return run_cli(["-i", path, "-t", "1", "-q", "1"] + list(args))
+
+
+def test_cli_tuner_is_deterministic_and_scores_with_the_batch(tmp_path, fixtures):
+    """-t 1: the reference's simulated-annealing tuner with one Metropolis chain per replica.
+    Its random draws come from one mt19937 seeded with -l, so a run repeats exactly; iteration
+    0 runs every replica with its original parameters, so its scores are the lowest loc of
+    each replica run alone to the step cap; the tuning file holds one line per new global."""
+    f = fixtures["n1000"]
+    form = dmm.from_arrays(f["lits"], f["off"], f["n"])
+    path = str(tmp_path / "n1000.cnf")
+    dmm.write_cnf(form, path)
+    args = ["-s", "4", "-z", "30", "-w", "3", "-l", "1"]
+    out = _tune(path, *args)
+    assert out == _tune(path, *args)
+    assert out.count("c [TUNE] ITERATION") == 4 and "c [TUNE] FINISHED." in out
+    decisions = re.findall(r"c \[TUNE\] \[(\d)\] (?:\d+ CANDIDATES ACCEPTED|CANDIDATE REJECTED) "
+                           r"\(E=(\d+)", out)
+    assert len(decisions) == 4 * 3
+    # iteration 0 against the library: replica r from its reference state, alpha / r
+    e0 = {int(r): int(e) for r, e in decisions[:3]}
+    for r in range(3):
+        x0, div = dmm.initial_state_reference(form, 1, r)
+        p = dmm.default_params()
+        p.alpha = p.alpha / div
+        b = dmm.Batch.for_formulas([form], precision="fp64")
+        try:
+            b.add(form, x0, params=p, max_steps=30)
+            b.run()
+            res, _ = b.result(0)
+        finally:
+            b.close()
+        assert e0[r] == res.best_loc
+    assert float(out.strip().splitlines()[-1]) == min(int(e) for _, e in decisions)
+    lines = open(path + ".tuning.txt").read().splitlines()
+    assert lines[0].startswith("ITERATION;INSTANCE;PARAM_01") and len(lines) >= 2
+
+
+def test_cli_tuner_stops_on_a_solution(tmp_path, fixtures):
+    f = fixtures["n100"]
+    path = str(tmp_path / "n100.cnf")
+    dmm.write_cnf(dmm.from_arrays(f["lits"], f["off"], f["n"]), path)
+    out = _tune(path, "-s", "50", "-z", "5000", "-w", "2", "-l", "0")
+    assert "c [TUNE] SOLUTION FOUND." in out and out.rstrip().endswith("0")
