@@ -11,7 +11,7 @@
 // production FP32 path.  Replicas (-w) start from the reference's per-replica initial
 // states with alpha / i (dynex.cc:2643-2700) and run together in one batch; the replica
 // that solves at the lowest step wins.  -p 1 runs the reference's alpha heuristic every
-// 10^4 steps (one replica).  Options of the reference that select modes outside the
+// 10^4 steps (with replicas, on each replica in turn).  Options of the reference that select modes outside the
 // default integrator (-o, -t, -e, ...) are accepted and reported as unsupported when they
 // ask for anything but the default.  -S 1 writes the final state of the reported replica
 // to <cnf>.assignment.txt in the reference's checkpoint format (dynex.cc:2131-2135); -L 1
@@ -472,83 +472,107 @@ int main(int argc, char** argv) {
   std::vector<int8_t> pre(n), post(n);
   int winner = 0;
   bool solved = false;
-  if (o.replicas == 1) {
-    dmm_instance* inst = nullptr;
-    int32_t div = 1;
-    if (fail(dmm_instance_create(cnf->lits, cnf->clause_off, n, m, o.prec, o.device, &inst),
-             "creating the instance") ||
-        fail(dmm_initial_state_reference(cnf->lits, cnf->clause_off, n, m, o.seed, 0, x.data(), &div),
-             "initial state") ||
-        fail(dmm_instance_set_params(inst, &o.p, nullptr), "parameters") ||
-        fail(x_loaded.empty() ? dmm_instance_set_state(inst, x.data())
-                              : dmm_instance_set_state_at(inst, x_loaded.data(), t_loaded, 0),
-             "state")) {
-      dmm_instance_destroy(inst);
-      dmm_cnf_free(cnf);
-      return EXIT_FAILURE;
-    }
-    if (!o.quiet) std::printf("c [0] STARTING ODE...\n");
-    bool ok = true;
-    if (!o.heuristics) {
-      dmm_limits lim{o.max_steps, 0, o.walltime};
-      ok = !fail(dmm_instance_solve(inst, &lim, &rep), "integration");
-    } else {
-      // integrate to every 10^4-th step, apply the heuristic to the state there, continue
-      std::vector<double> acm((size_t)m, o.p.alpha);  // dmm_alpha_cm (dynex.cc:1201)
-      const double xl_max = effective_xl_max(o.p.xl_max, m);
-      ok = !fail(dmm_instance_set_params(inst, &o.p, acm.data()), "parameters");
-      while (ok) {
-        dmm_report cur{};
-        ok = !fail(dmm_instance_report(inst, &cur), "report");
-        int target = (cur.steps / kHeuristicEvery + 1) * kHeuristicEvery;
-        if (o.max_steps > 0) target = std::min(target, o.max_steps);
-        double wall = 0.0;
-        if (o.walltime > 0) {
-          wall = o.walltime - (now_s() - t0);
-          if (wall <= 0) break;
+  if (o.replicas == 1 || o.heuristics) {
+    // One replica, or replicas with the alpha heuristic (which needs each replica's state
+    // every 10^4 steps): every replica on its own instance, one after another.  A later
+    // replica runs at most to the best solving step so far (only an earlier solve wins), and
+    // each replica has the whole wall-time limit, as each of the reference's threads has.
+    dmm_instance* keep = nullptr;
+    auto drop = [&](dmm_instance* i) { dmm_instance_destroy(i); };
+    for (int r = 0; r < o.replicas; r++) {
+      dmm_instance* inst = nullptr;
+      int32_t div = 1;
+      dmm_params pr = o.p;
+      const bool set_up =
+          !fail(dmm_instance_create(cnf->lits, cnf->clause_off, n, m, o.prec, o.device, &inst),
+                "creating the instance") &&
+          !fail(dmm_initial_state_reference(cnf->lits, cnf->clause_off, n, m, o.seed, r, x.data(),
+                                            &div), "initial state");
+      pr.alpha = o.p.alpha / div;  // dynex.cc:2657
+      if (!set_up || fail(dmm_instance_set_params(inst, &pr, nullptr), "parameters") ||
+          fail(x_loaded.empty() ? dmm_instance_set_state(inst, x.data())
+                                : dmm_instance_set_state_at(inst, x_loaded.data(), t_loaded, 0),
+               "state")) {
+        drop(inst);
+        drop(keep);
+        dmm_cnf_free(cnf);
+        return EXIT_FAILURE;
+      }
+      int cap = o.max_steps;
+      if (solved) cap = cap > 0 ? std::min(cap, rep.solved_step) : rep.solved_step;
+      if (!o.quiet) std::printf("c [%d] STARTING ODE...\n", r);
+      const double tr = now_s();
+      dmm_report rr{};
+      bool ok = true;
+      if (!o.heuristics) {
+        dmm_limits lim{cap, 0, o.walltime};
+        ok = !fail(dmm_instance_solve(inst, &lim, &rr), "integration");
+      } else {
+        // integrate to every 10^4-th step, apply the heuristic to the state there, continue
+        std::vector<double> acm((size_t)m, pr.alpha);  // dmm_alpha_cm (dynex.cc:1201)
+        const double xl_max = effective_xl_max(o.p.xl_max, m);
+        ok = !fail(dmm_instance_set_params(inst, &pr, acm.data()), "parameters");
+        while (ok) {
+          dmm_report cur{};
+          ok = !fail(dmm_instance_report(inst, &cur), "report");
+          int target = (cur.steps / kHeuristicEvery + 1) * kHeuristicEvery;
+          if (cap > 0) target = std::min(target, cap);
+          double wall = 0.0;
+          if (o.walltime > 0) {
+            wall = o.walltime - (now_s() - tr);
+            if (wall <= 0) break;
+          }
+          dmm_limits lim{target, 0, wall};
+          if (!ok || fail(dmm_instance_solve(inst, &lim, &rr), "integration")) {
+            ok = false;
+            break;
+          }
+          if (rr.status != DMM_STEP_LIMIT || rr.steps != target || (cap > 0 && rr.steps >= cap))
+            break;  // solved, out of time, or at the step cap
+          double t = 0.0;
+          if (fail(dmm_instance_get_state(inst, x.data(), &t), "state")) {
+            ok = false;
+            break;
+          }
+          // floor: the replica's alpha; Xl reset: -c (dynex.cc:1446-1450)
+          const HeuristicCounts hc = alpha_heuristic(x, acm, n, m, pr.alpha, o.p.alpha, xl_max);
+          std::printf("c [%d] alpha heuristic changed %d up, %d down, %d max reached (median = %.2f)\n",
+                      r, hc.up, hc.down, hc.max, hc.median);
+          ok = !fail(dmm_instance_set_params(inst, &pr, acm.data()), "parameters") &&
+               !fail(dmm_instance_set_state_at(inst, x.data(), t, rr.steps), "state");
         }
-        dmm_limits lim{target, 0, wall};
-        if (!ok || fail(dmm_instance_solve(inst, &lim, &rep), "integration")) {
-          ok = false;
-          break;
-        }
-        if (rep.status != DMM_STEP_LIMIT || rep.steps != target ||
-            (o.max_steps > 0 && rep.steps >= o.max_steps))
-          break;  // solved, out of time, or at the step cap
-        double t = 0.0;
-        if (fail(dmm_instance_get_state(inst, x.data(), &t), "state")) {
-          ok = false;
-          break;
-        }
-        const HeuristicCounts hc = alpha_heuristic(x, acm, n, m, o.p.alpha, o.p.alpha, xl_max);
-        std::printf("c [0] alpha heuristic changed %d up, %d down, %d max reached (median = %.2f)\n",
-                    hc.up, hc.down, hc.max, hc.median);
-        ok = !fail(dmm_instance_set_params(inst, &o.p, acm.data()), "parameters") &&
-             !fail(dmm_instance_set_state_at(inst, x.data(), t, rep.steps), "state");
+      }
+      if (!ok) {
+        drop(inst);
+        drop(keep);
+        dmm_cnf_free(cnf);
+        return EXIT_FAILURE;
+      }
+      const bool won = rr.status == DMM_SOLVED && (!solved || rr.solved_step < rep.solved_step);
+      if (r == 0 || won) {
+        drop(keep);
+        keep = inst;
+        rep = rr;
+        winner = r;
+        solved = rr.status == DMM_SOLVED;
+      } else {
+        drop(inst);
       }
     }
-    if (!ok) {
-      dmm_instance_destroy(inst);
-      dmm_cnf_free(cnf);
-      return EXIT_FAILURE;
-    }
-    solved = rep.status == DMM_SOLVED;
     double t_end = 0.0;
-    if (fail(dmm_instance_assignment(inst, solved ? pre.data() : nullptr, post.data()),
+    if (fail(dmm_instance_assignment(keep, solved ? pre.data() : nullptr, post.data()),
              "assignment") ||
-        (o.save_state && (fail(dmm_instance_get_state(inst, x.data(), &t_end), "state") ||
+        (o.save_state && (fail(dmm_instance_get_state(keep, x.data(), &t_end), "state") ||
                           fail(dmm_state_write(state_file.c_str(), x.data(), n, m, t_end),
                                "writing the state")))) {
-      dmm_instance_destroy(inst);
+      drop(keep);
       dmm_cnf_free(cnf);
       return EXIT_FAILURE;
     }
-    dmm_instance_destroy(inst);
+    drop(keep);
   } else {
     dmm_batch* b = nullptr;
     const int R = o.replicas;
-    if (o.heuristics)
-      std::fprintf(stderr, "c -p: the alpha heuristic runs with one replica (-w 1) only\n");
     if (fail(dmm_batch_create(o.prec, o.device, R, (int64_t)n * R, (int64_t)m * R,
                               cnf->nlits * R, &b), "creating the batch")) {
       dmm_cnf_free(cnf);

@@ -183,3 +183,28 @@ def test_cli_tuner_stops_on_a_solution(tmp_path, fixtures):
     dmm.write_cnf(dmm.from_arrays(f["lits"], f["off"], f["n"]), path)
     out = _tune(path, "-s", "50", "-z", "5000", "-w", "2", "-l", "0")
     assert "c [TUNE] SOLUTION FOUND." in out and out.rstrip().endswith("0")
+
+
+def test_cli_alpha_heuristic_with_replicas(tmp_path, known_answers):
+    """-p 1 -w 2: each replica runs the heuristic on its own state and clause alphas (floor:
+    the replica's alpha).  Replica 0 runs first and unchanged, so its heuristic lines are the
+    reference's one-replica lines; replica 1 runs at most to replica 0's solving step, and
+    the reported solve is the earlier one."""
+    ka = known_answers["cli_heuristics"]
+    f = ka["formula"]
+    form, _ = dmm.generate_planted(f["n"], f["m"], f["p0"], f["p1"], seed=f["seed"])
+    path = str(tmp_path / "heuristics.cnf")
+    dmm.write_cnf(form, path)
+    text = run_cli(["-i", path, "-p", "1", "-w", "2"], timeout=600)
+    lines = re.findall(r"c \[(\d)\] alpha heuristic changed (\d+) up, (\d+) down, (\d+) max "
+                       r"reached \(median = ([0-9.]+)\)", text)
+    r0 = [[int(a), int(b), int(c), d] for k, a, b, c, d in lines if k == "0"]
+    assert r0 == ka["heuristics"]
+    assert all(k in "01" for k, *_ in lines)
+    out = parse(text)
+    assert out["sat"] and out["verified"]
+    winner = int(re.search(r"s \[(\d)\] SATISFIABLE", text).group(1))
+    if winner == 0:
+        assert out["steps"] == ka["steps"] and out["T"] == pytest.approx(ka["T"], abs=1e-9)
+    else:
+        assert out["steps"] < ka["steps"]
