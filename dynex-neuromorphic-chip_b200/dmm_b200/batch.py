@@ -67,6 +67,16 @@ class Batch:
                                      ptr(post, ctypes.c_int8)))
         return Result.from_report(r), post
 
+    def set_state_at(self, index: int, x, t: float, step: int = 0) -> None:
+        """Restarts formula `index` from state x at time t after `step` steps (a resume
+        from a checkpoint, dynex.cc:2521-2532)."""
+        f = self.formulas[index]
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.shape != (f.state_size(),):
+            raise ValueError("x must have n + 2m entries")
+        check(lib().dmm_batch_set_state_at(self._h, int(index), ptr(x, ctypes.c_double),
+                                           float(t), int(step)))
+
     def state(self, index: int):
         f = self.formulas[index]
         x = np.zeros(f.state_size(), dtype=np.float64)

@@ -221,3 +221,34 @@ def test_staged_kernel_limits(n, m, form_want):
             outs.append((inst.get_state()[0], rep.t, rep.loc, rep.energy))
     assert np.array_equal(outs[0][0], outs[1][0])
     assert outs[0][1:] == outs[1][1:]
+
+
+def test_batch_resume_from_checkpoint_equals_instance(tmp_path, fixtures):
+    """A state checkpoint written after 40 steps and read back resumes a batch member exactly
+    as it resumes a lone instance (FP64: same steps, time, best loc and final state)."""
+    f = fixtures["n500"]
+    form = formula(f)
+    x0, _ = dmm.initial_state_reference(form, 2, 0)
+    with dmm.Instance(form, precision="fp64") as inst:
+        inst.set_state(x0)
+        inst.step(40)
+        x, t = inst.get_state()
+    path = str(tmp_path / "n500.cnf.assignment.txt")
+    dmm.write_state(path, x, form.n, form.m, t)
+    xr, tr = dmm.read_state(path, form.n, form.m)
+    with dmm.Instance(form, precision="fp64") as inst:
+        inst.set_state_at(xr, tr, 0)
+        want = inst.solve(max_steps=60)
+        want_x = inst.get_state()[0]
+    b = dmm.Batch.for_formulas([form], precision="fp64")
+    try:
+        b.add(form, x0, max_steps=60)
+        b.set_state_at(0, xr, tr, 0)
+        b.run()
+        got, _ = b.result(0)
+        got_x = b.state(0)[0]
+    finally:
+        b.close()
+    assert (got.status, got.steps, got.t, got.best_loc) == (want.status, want.steps, want.t,
+                                                             want.best_loc)
+    assert np.array_equal(got_x, want_x)
