@@ -480,6 +480,7 @@ int main(int argc, char** argv) {
     dmm_instance* keep = nullptr;
     auto drop = [&](dmm_instance* i) { dmm_instance_destroy(i); };
     for (int r = 0; r < o.replicas; r++) {
+      if (solved && rep.solved_step <= 0) break;  // solved by an initial state: nothing is earlier
       dmm_instance* inst = nullptr;
       int32_t div = 1;
       dmm_params pr = o.p;
