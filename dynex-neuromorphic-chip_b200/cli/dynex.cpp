@@ -146,7 +146,7 @@ double now_s() {
 // std::mt19937 seeded with -l, the same distributions drawn in the same order), so the
 // parameter sequence depends only on the objectives.  Each iteration runs all replicas as one
 // batch on the GPU, each to the step cap (-z) or its solution; the reference's threads also
-// stop when any of them solves, a race this build does not reproduce.  The initial objective
+// stop when any of them solves, a race that is not reproduced here.  The initial objective
 // is the loc of each replica's initial state (the reference takes one Euler step through
 // odeint, dynex.cc:1711-1716, whose one right-hand side sees that state).
 struct TuneOpts {

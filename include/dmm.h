@@ -134,7 +134,7 @@ const char* dmm_status_string(dmm_status s);
 /* Text of the last error raised on the calling thread ("" if none). */
 const char* dmm_last_error(void);
 void dmm_params_default(dmm_params* p);
-/* Number of CUDA devices usable by this build (0 when none). */
+/* Number of CUDA devices this library can use (0 when none). */
 int32_t dmm_device_count(void);
 /* No counterpart in the reference.  Instances and batches take their device buffers from a
  * process-wide cache: a destroyed instance's buffers are kept (up to 8 GiB per device) and
