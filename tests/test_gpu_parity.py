@@ -251,3 +251,37 @@ def test_edge_formulas():
     with dmm.Instance(form, precision="fp64") as inst:
         rows, _ = run_steps(inst, x0, 50)
     assert np.array_equal(rows, ref["dump"][: ref["steps"] + 1])
+
+
+def test_lists_longer_than_the_device_sorter():
+    """A variable in 3000 clauses: its occurrence list is longer than the device sorter takes
+    (1024), so it is sorted on the host before the first step, for a lone instance and for
+    two formulas added to one batch (both recorded before one commit).  FP64 states equal
+    the oracle's bit for bit."""
+    rng = np.random.default_rng(11)
+    n, m = 50, 3000
+    rows = []
+    for c in range(m):
+        vs = np.concatenate([[1], rng.choice(np.arange(2, n + 1), size=2, replace=False)])
+        rows.append(vs * rng.choice([-1, 1], size=3))
+    lits = np.array(rows, np.int32).reshape(-1)
+    off = np.arange(0, 3 * m + 1, 3, dtype=np.int64)
+    form = dmm.from_arrays(lits, off, n)
+    assert form.max_occurrence == m
+    o = Oracle(n, m, lits, off)
+    x0, _ = dmm.initial_state_reference(form, 3)
+    ref = o.run(x0, 40, dump_every=1)
+    with dmm.Instance(form, precision="fp64") as inst:
+        got, _ = run_steps(inst, x0, 40)
+    assert np.array_equal(got, ref["dump"][: ref["steps"] + 1])
+    b = dmm.Batch(3, 3 * n, 3 * m, 9 * m, precision="fp64")
+    try:
+        b.add(form, x0, max_steps=40)
+        b.add(form, x0, max_steps=40)
+        b.run()
+        for k in range(2):
+            res, _ = b.result(k)
+            assert res.steps == ref["steps"]
+            assert np.array_equal(b.state(k)[0], ref["dump"][ref["steps"]])
+    finally:
+        b.close()
