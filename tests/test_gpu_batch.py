@@ -252,3 +252,23 @@ def test_batch_resume_from_checkpoint_equals_instance(tmp_path, fixtures):
     assert (got.status, got.steps, got.t, got.best_loc) == (want.status, want.steps, want.t,
                                                              want.best_loc)
     assert np.array_equal(got_x, want_x)
+
+
+@pytest.mark.parametrize("m", [976_211, 976_797])
+def test_staged_clause_rounds_with_ragged_tiles(m):
+    """The staged kernel's clause rounds: 4-clause groups per thread, then a remainder of at
+    most 2 x 1024 clauses as pairs (m = 976,211: the last tile has an odd remainder, one
+    clause alone) or, above that, as groups again (m = 976,797: 6,600-clause tiles and a last
+    tile of 6,597, whose remainder ends with one clause alone).  First 4 steps bit-exact
+    against the oracle's FP32 restatement."""
+    n = m // 8
+    form, _ = dmm.generate_planted(n, m, p0=0.08, p1=0.46, seed=m)
+    x0 = dmm.initial_state_uniform(form, 5)
+    o = Oracle(form.n, form.m, form.lits, form.clause_off, precision="fp32")
+    ref = o.run(x0, 4, dump_every=2)
+    with dmm.Instance(form, precision="fp32") as inst:
+        assert inst.launch_form == "staged"
+        inst.set_state(x0)
+        for r in range(1, 3):
+            inst.step(2)
+            assert np.array_equal(inst.get_state()[0], ref["dump"][r])
