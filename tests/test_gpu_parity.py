@@ -285,3 +285,18 @@ def test_lists_longer_than_the_device_sorter():
             assert np.array_equal(b.state(k)[0], ref["dump"][ref["steps"]])
     finally:
         b.close()
+
+
+def test_fp64_many_variable_tiles_per_block():
+    """FP64 with 32-variable tiles at n = 6,000 (188 tiles, more than one per block, the
+    sorted sums' group counter restarting for each): bit-exact against the oracle."""
+    form, _ = dmm.generate_planted(6_000, 25_200, 0.08, 0.46, seed=12)
+    o = Oracle(form.n, form.m, form.lits, form.clause_off)
+    x0 = uniform_init(form.n, form.m, 4)
+    ref = o.run(x0, 30, dump_every=10)
+    with dmm.Instance(form, precision="fp64") as inst:
+        inst.set_tuning(var_tile=32, clause_tile=256)
+        inst.set_state(x0)
+        for r in range(1, 4):
+            inst.step(10)
+            assert np.array_equal(inst.get_state()[0], ref["dump"][r])
