@@ -114,3 +114,21 @@ def test_oracle_planted_fixtures_verify(fixtures):
         f = fixtures[name]
         o = Oracle(f["n"], f["m"], f["lits"], f["off"])
         assert o.check(f["planted"]) == 0
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference harness not built")
+def test_oracle_long_occurrence_list_vs_reference():
+    """A variable in every one of 3000 clauses (its sorted sum runs over 3000 entries)."""
+    rng = np.random.default_rng(11)
+    n, m = 50, 3000
+    rows = [np.concatenate([[1], rng.choice(np.arange(2, n + 1), size=2, replace=False)])
+            * rng.choice([-1, 1], size=3) for _ in range(m)]
+    lits = np.array(rows, np.int32).reshape(-1)
+    off = np.arange(0, 3 * m + 1, 3, dtype=np.int64)
+    o = Oracle(n, m, lits, off)
+    ref = Reference(n, m, lits, off)
+    x0 = o.init_state(3)
+    a = o.run(x0, 40, dump_every=1)
+    b = ref.run(x0, 40, dump_every=1)
+    assert np.array_equal(a["dump"], b["dump"])
+    assert np.array_equal(a["loc"], b["loc"])
