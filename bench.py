@@ -41,9 +41,10 @@ N_VARS, N_CLAUSES, P0, P1 = 100_000, 800_000, 0.08, 0.46
 INSTANCE_SEED, INIT_SEED = 1, 1001
 FLUSH_BYTES = 256 << 20
 METRIC = "clause-updates/s"
-WORKLOAD = "planted 3-SAT n=100000 m=800000 r=8 p0=0.08 (plain single instance, FP32)"
+WORKLOAD = "planted 3-SAT n=100000 m=800000 r=8 p0=0.08 p1=0.46, one formula per GPU"
 E2E_STEPS = 64
 CPU_SAMPLE_STEPS = 60
+LARGE_N, LARGE_SEED = 1_000_000, 3
 
 
 def parse():
@@ -53,6 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--procs", type=int, default=0,
+                    help="reference arm: host processes (default: one per core)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and served workloads (rank 0, one GPU)")
     ap.add_argument("--precision-study", action="store_true",
@@ -62,6 +65,8 @@ def parse():
     ap.add_argument("--study-ratio", type=float, default=8.0,
                     help="clause-to-variable ratio of the study's formula")
     ap.add_argument("--study-max-steps", type=int, default=5000)
+    ap.add_argument("--no-study", action="store_true",
+                    help="leave the precision study out of the default run")
     return ap.parse_args()
 
 
@@ -95,11 +100,20 @@ def run_extras(device: int) -> dict:
                          "clause_updates_per_s": p["clause_updates_per_s"],
                          "path": "dmm_instance create + solve, one formula at a time"},
         "batched_same_sample_solves_per_s": pb["solves_per_s_run"],
+        "batched_same_sample_solves_per_s_incl_setup": pb["solves_per_s"],
         "autotune": {"best": tuned["best"],
                      "sample_device_ms": {f"var_group={g},steps_per_graph={sp}": round(ms, 3)
                                           for (g, sp), ms in tuned["table"]},
                      "note": "first 512 formulas, each shape; results identical for every shape"},
-        "solves_ratio_vs_plain": b["solves_per_s_run"] / max(p["solves_per_s"], 1e-9),
+        # set-up (formula upload, device CSR build, initial state) is inside both rates
+        "solves_ratio_vs_plain": b["solves_per_s"] / max(p["solves_per_s"], 1e-9),
+        "solves_ratio_vs_plain_run_only": b["solves_per_s_run"] / max(p["solves_per_s"], 1e-9),
+        "roofline": roofline(
+            sum((28 * it.formula.m + 8 * it.formula.n) * st for it, st in zip(items, b["steps"])),
+            b["device_ms"], "k_inst (one block per formula, many steps per launch)",
+            traffic=None,
+            note="algorithmic bytes (28m + 8n per accepted step) of every formula's steps over "
+                 "the run's device time"),
     }
     sv = w.make_items(300, 100, 100000, ratios=(4.3, 6.0, 8.0), seed=2)
     arr = w.poisson_times(len(sv), 200.0, seed=2)
@@ -184,10 +198,10 @@ KERNELS = {"staged": "k_staged (fused step, staged form)",
            "two-kernel": "k_clause + k_var", "one-block-per-formula": "k_inst"}
 
 
-def profiled_traffic() -> float | None:
-    """DRAM bytes per launch of the step kernel at this workload, from the committed ncu
-    summary (profiles/k_staged_n100k.md, line `traffic_bytes_per_launch: X`)."""
-    p = os.path.join(ROOT, "profiles", "k_staged_n100k.md")
+def profiled_traffic(summary: str) -> float | None:
+    """DRAM bytes per launch of a step kernel, from a committed ncu summary under profiles/
+    (its line `traffic_bytes_per_launch: X`); None when there is none."""
+    p = os.path.join(ROOT, "profiles", summary)
     try:
         with open(p) as f:
             m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read())
@@ -204,58 +218,88 @@ def make_instance(rank: int):
     return form, x0
 
 
+def bench_config(world: int) -> dict:
+    """The workload description both arms print (the reference arm's line must carry the
+    same config as this one's)."""
+    return {"workload": WORKLOAD, "n": N_VARS, "m": N_CLAUSES, "instance_seed": INSTANCE_SEED,
+            "init_seed": INIT_SEED, "per_gpu_instances": 1,
+            "l2": "GPU arm: flushed (256 MiB write) before every timed step; CPU reference "
+                  "arm: no flush (its working set exceeds the host caches)",
+            "parallelism": f"replicas x{world}"}
+
+
 # ---- reference arm (CPU) ------------------------------------------------------------------
 
 def _ref_worker(args):
-    rank, steps, warmup = args
-    import numpy as np  # noqa: F401
+    """One host process: the instance and initial state built by the reference harness
+    library (no other native library is loaded), then `warmup` untimed and `steps` timed
+    accepted steps of the reference's own right-hand side and Euler step."""
+    steps, warmup = args
+    from oracle.oracle import Reference, planted_instance
 
-    from oracle.oracle import Reference
-
-    form, x0 = make_instance(rank)
-    ref = Reference(form.n, form.m, form.lits, form.clause_off)
+    lits, off, _, x0 = planted_instance(N_VARS, N_CLAUSES, P0, P1, INSTANCE_SEED, INIT_SEED)
+    ref = Reference(N_VARS, N_CLAUSES, lits, off)
     if warmup:
         ref.run(x0, warmup)
     t0 = time.perf_counter()
     r = ref.run(x0, steps)
     dt = time.perf_counter() - t0
-    return r["steps"], dt
+    return r["steps"], dt, repo_libraries()
+
+
+def repo_libraries() -> list[str]:
+    """Shared libraries of this repository mapped into the calling process (Linux)."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(ROOT + os.sep):
+                    found.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(found)
 
 
 def cpu_reference(steps: int, warmup: int, procs: int):
     """The unmodified reference integrator (oracle/_ref, dynex.cc's own right-hand side and
-    Euler step) on `procs` host processes at once, each on its own instance."""
+    Euler step) on `procs` host processes at once, all on the bench instance and initial
+    state; returns (clause-updates/s over the slowest process, details)."""
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
         t0 = time.perf_counter()
-        res = pool.map(_ref_worker, [(r, steps, warmup) for r in range(procs)])
+        res = pool.map(_ref_worker, [(steps, warmup)] * procs)
         wall = time.perf_counter() - t0
-    done = sum(s for s, _ in res)
-    t = max(d for _, d in res)
-    return N_CLAUSES * done / t, {"procs": procs, "steps_each": steps, "timed_s": t,
-                                  "wall_s": wall}
+    done = sum(r[0] for r in res)
+    t = max(r[1] for r in res)
+    libs = sorted({x for r in res for x in r[2]})
+    return N_CLAUSES * done / t, {"procs": procs, "steps_each": [r[0] for r in res],
+                                  "timed_s": t, "wall_s": wall, "libraries": libs}
 
 
 def run_reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    procs = max(1, os.cpu_count() or 1)
-    steps = max(1, a.steps // 4)
-    value, info = cpu_reference(steps, 0, procs)
+    procs = a.procs or max(1, os.cpu_count() or 1)
+    steps, warmup = a.steps, max(3, a.warmup)
+    value, info = cpu_reference(steps, warmup, procs)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "clause-updates/s",
-        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "n_gpus": a.gpus, "steps": steps, "warmup": warmup,
         "ms_per_step": 1000.0 * info["timed_s"] / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD.replace("FP32", "FP64 reference CPU"),
-                   "l2": "n/a (CPU)"},
+        "config": bench_config(a.gpus),
         "cpu_baseline": {"value": value, "unit": "clause-updates/s", "cores": procs,
                          "kind": "reference",
-                         "sample": f"{procs} processes x {steps} steps of the n=100000 "
-                                   "instance (each process its own seed)"},
+                         "sample": f"{procs} processes, each {warmup} untimed + {steps} timed "
+                                   "steps of the bench instance and initial state (the "
+                                   "unmodified dynex.cc right-hand side and Euler step with "
+                                   "its adaptive loop, one thread each)"},
         "e2e": {"value": value, "unit": "clause-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "steps_done_per_process": info["steps_each"],
+        "repo_libraries_loaded": info["libraries"],
     }
     print(json.dumps(line), flush=True)
 
@@ -313,6 +357,134 @@ class Ranks:
             self.dist = None
 
 
+def time_plain(inst, x0, K, W, ranks, barrier, clocks_gpu=None):
+    """Device time of K steps of `inst` from x0, each launched alone after an L2 flush (W
+    untimed steps first), restarting from a later initial state when a replica solved
+    inside the timed region (every rank takes the same collective decision).  Returns
+    (ms, steps done, clocks summary or None, x0 used)."""
+    import dmm_b200 as dmm
+
+    f = inst.formula
+    init_seed = INIT_SEED
+    clocks = None
+    for attempt in range(4):
+        inst.set_state(x0)
+        inst.time_steps_flushed(W, FLUSH_BYTES)  # warm-up: the same launches as timed
+        barrier()
+        s0 = inst.report().steps
+        if clocks_gpu is not None:
+            with Clocks(clocks_gpu) as clk:
+                step_ms = inst.time_steps_flushed(K, FLUSH_BYTES)
+            clocks = clk.summary()
+        else:
+            step_ms = inst.time_steps_flushed(K, FLUSH_BYTES)
+        barrier()
+        steps_done = inst.report().steps - s0
+        if not ranks.any(steps_done != K):
+            break
+        init_seed += 1000
+        x0 = dmm.initial_state_uniform(f, init_seed)
+    return step_ms, steps_done, clocks, x0
+
+
+def time_resident(inst, x0, K, W):
+    """K steps on the solver's own launch path (cooperative launches of several steps each,
+    no flush); returns (ms, steps)."""
+    inst.set_state(x0)
+    inst.time_steps(W)
+    s0 = inst.report().steps
+    ms = inst.time_steps(K)
+    return ms, inst.report().steps - s0
+
+
+def time_e2e(form, x0, precision, device, barrier, reps=7):
+    """Create + state upload + E2E_STEPS steps + assignment readback through the C ABI from
+    pinned host buffers; median wall time of `reps` calls after 2 untimed ones."""
+    import torch
+
+    import dmm_b200 as dmm
+
+    lits_p = torch.from_numpy(form.lits).pin_memory()
+    off_p = torch.from_numpy(form.clause_off).pin_memory()
+    x0_p = torch.from_numpy(x0).pin_memory()
+    pform = dmm.Formula(form.n, form.m, lits_p.numpy(), off_p.numpy(), form.max_occurrence)
+    times, steps = [], []
+    for it in range(2 + reps):
+        barrier()
+        t0 = time.perf_counter()
+        with dmm.Instance(pform, precision=precision, device=device) as e:
+            e.set_state(x0_p.numpy())
+            r = e.step(E2E_STEPS)
+            _, post = e.assignment(pre=False)
+        dt = time.perf_counter() - t0
+        if it >= 2:
+            times.append(dt)
+            steps.append(r.steps)
+    h2d = form.lits.nbytes + form.clause_off.nbytes + x0.nbytes
+    d2h = form.n + 56
+    return statistics.median(times), statistics.median(steps), h2d, d2h
+
+
+def roofline(algo_bytes_per_launch, launch_ms, kernel, traffic=None, note=None):
+    peak, peak_kind = peaks()
+    achieved = algo_bytes_per_launch / (launch_ms / 1000.0) / 1e9
+    r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+         "frac": achieved / peak, "traffic": traffic, "kernel": kernel, "peak_kind": peak_kind,
+         "algo_bytes_per_launch": algo_bytes_per_launch}
+    if traffic:
+        r["traffic_over_algo"] = traffic / algo_bytes_per_launch
+    if note:
+        r["note"] = note
+    return r
+
+
+def fp64_line(form, x0, K, W, device, ranks, barrier) -> dict:
+    """The same formula and state in FP64, the reference's arithmetic (bit-exact): the
+    like-for-like comparison with the reference's precision."""
+    import dmm_b200 as dmm
+
+    n, m = form.n, form.m
+    with dmm.Instance(form, precision="fp64", device=device) as inst:
+        kern = KERNELS[inst.launch_form]
+        ms, done, _, xs = time_plain(inst, x0, K, W, ranks, barrier)
+        rms, rsteps = time_resident(inst, xs, K, W)
+    e_t, e_steps, h2d, d2h = time_e2e(form, x0, "fp64", device, barrier, reps=5)
+    algo = 44 * m + 16 * n  # literals 12m, Xs/Xl read+write 32m, V read 8n + write 8n
+    return {"value": m * done / (ms / 1000.0), "unit": "clause-updates/s",
+            "ms_per_step": ms / K, "dtype": "f64",
+            "resident": {"value": m * rsteps / (rms / 1000.0), "ms_per_step": rms / max(1, rsteps)},
+            "e2e": {"value": m * e_steps / e_t, "unit": "clause-updates/s",
+                    "h2d_bytes_per_step": h2d / E2E_STEPS, "d2h_bytes_per_step": d2h / E2E_STEPS},
+            "roofline": roofline(algo, ms / K, kern,
+                                 traffic=profiled_traffic("k_persist_fp64_n100k.md"))}
+
+
+def large_line(K, W, device, ranks, barrier) -> dict:
+    """Plain single formula at n = 1,000,000, m = 8,000,000 (FP32), whose per-step working set
+    (2.3e8 algorithmic bytes) exceeds the 126 MB L2: the configuration where the step is
+    bound by HBM."""
+    import dmm_b200 as dmm
+
+    n, m = LARGE_N, LARGE_N * 8
+    f, _ = dmm.generate_planted(n, m, P0, P1, seed=LARGE_SEED)
+    x0 = dmm.initial_state_uniform(f, LARGE_SEED + 1000)
+    out = {"workload": f"planted 3-SAT n={n} m={m} r=8 p0=0.08 p1=0.46, one formula, FP32",
+           "n": n, "m": m}
+    with dmm.Instance(f, precision="fp32", device=device) as inst:
+        kern = KERNELS[inst.launch_form]
+        out["launch_form"] = inst.launch_form
+        ms, done, _, xs = time_plain(inst, x0, K, W, ranks, barrier)
+        rms, rsteps = time_resident(inst, xs, K, W)
+    algo = 28 * m + 8 * n
+    out.update({"value": m * done / (ms / 1000.0), "unit": "clause-updates/s",
+                "ms_per_step": ms / K,
+                "resident": {"value": m * rsteps / (rms / 1000.0),
+                             "ms_per_step": rms / max(1, rsteps)},
+                "roofline": roofline(algo, ms / K, kern,
+                                     traffic=profiled_traffic("k_staged_n1m.md"))})
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -327,7 +499,6 @@ def main():
                           f"r={a.study_ratio:g}, p0=0.08, FP32 vs FP64 from the same initial "
                           "states"}), flush=True)
         return
-    import numpy as np
     import torch
 
     import dmm_b200 as dmm
@@ -345,23 +516,7 @@ def main():
     K, W = a.steps, max(3, a.warmup)
     inst = dmm.Instance(form, precision="fp32", device=local)
     form_name = inst.launch_form
-    init_seed = INIT_SEED + rank
-    for attempt in range(4):
-        inst.set_state(x0)
-        inst.time_steps_flushed(W, FLUSH_BYTES)  # warm-up: the same launches as timed
-        barrier()
-        s0 = inst.report().steps
-        with Clocks(local) as clk:
-            step_ms = inst.time_steps_flushed(K, FLUSH_BYTES)
-        barrier()
-        steps_done = inst.report().steps - s0
-        # a replica that solved inside the timed region did no-op steps: every rank restarts
-        # (the decision is collective, so all ranks take the same barriers)
-        if not ranks.any(steps_done != K):
-            break
-        init_seed += 1000
-        x0 = dmm.initial_state_uniform(form, init_seed)
-    clocks = clk.summary()
+    step_ms, steps_done, clocks, x0 = time_plain(inst, x0, K, W, ranks, barrier, local)
     t_max = max_over_ranks(step_ms)
     total_updates = sum_over_ranks(m * steps_done)
     value = total_updates / (t_max / 1000.0)
@@ -374,82 +529,66 @@ def main():
     clause_ms, var_ms = inst.profile(K, FLUSH_BYTES)
     inst.set_tuning(**tun)
 
-    # resident: the solver's own launch path (one cooperative launch per steps_per_graph
-    # steps, no flush; this instance's 4.2e7-byte working set stays in the 126 MB L2)
-    inst.set_state(x0)
-    inst.time_steps(W)
-    s0 = inst.report().steps
-    res_ms = inst.time_steps(K)
-    res_steps = inst.report().steps - s0
+    # resident: the solver's own launch path (cooperative launches of steps_per_graph steps
+    # each, no flush; this formula's 4.2e7-byte working set stays in the 126 MB L2)
+    res_ms, res_steps = time_resident(inst, x0, K, W)
     resident_value = sum_over_ranks(m * res_steps) / (max_over_ranks(res_ms) / 1000.0)
 
     # end to end through the C ABI from pinned host buffers
-    lits_p = torch.from_numpy(form.lits).pin_memory()
-    off_p = torch.from_numpy(form.clause_off).pin_memory()
-    x0_p = torch.from_numpy(x0).pin_memory()
-    pform = dmm.Formula(n, m, lits_p.numpy(), off_p.numpy(), form.max_occurrence)
-    e2e_times, e2e_steps = [], []
-    for it in range(2 + 7):
-        barrier()
-        t0 = time.perf_counter()
-        with dmm.Instance(pform, precision="fp32", device=local) as e:
-            e.set_state(x0_p.numpy())
-            r = e.step(E2E_STEPS)
-            _, post = e.assignment(pre=False)
-        dt = time.perf_counter() - t0
-        if it >= 2:
-            e2e_times.append(dt)
-            e2e_steps.append(r.steps)
-    e2e_t = max_over_ranks(statistics.median(e2e_times))
-    e2e_value = sum_over_ranks(m * statistics.median(e2e_steps)) / e2e_t
-    h2d = form.lits.nbytes + form.clause_off.nbytes + x0.nbytes
-    d2h = n + 56
+    e2e_med, e2e_steps, h2d, d2h = time_e2e(form, x0, "fp32", local, barrier)
+    e2e_t = max_over_ranks(e2e_med)
+    e2e_value = sum_over_ranks(m * e2e_steps) / e2e_t
 
-    peak, peak_kind = peaks()
     algo_bytes = 28 * m + 8 * n  # per step: literals 12m, Xs/Xl read+write 16m, V 4n + 4n
     launch_ms = t_max / K  # one cooperative launch = one step
-    achieved = algo_bytes / (launch_ms / 1000.0) / 1e9
-    traffic = profiled_traffic()
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, info = cpu_reference(CPU_SAMPLE_STEPS, 0, 1)
+        v, info = cpu_reference(CPU_SAMPLE_STEPS, 3, 1)
         cpu = {"value": v, "unit": "clause-updates/s", "cores": 1, "kind": "reference",
-               "sample": f"{CPU_SAMPLE_STEPS} steps of the same instance and initial state, "
-                         "reference dynex.cc right-hand side + Euler step, 1 thread"}
+               "sample": f"{CPU_SAMPLE_STEPS} steps (after 3 untimed) of the same formula and "
+                         "initial state, the unmodified dynex.cc right-hand side and Euler step "
+                         "with its adaptive loop, 1 thread"}
 
-    extras = None
+    extras = {}
     if rank == 0 and world == 1 and not a.no_extras:
-        extras = run_extras(local)
+        extras["fp64"] = fp64_line(form, x0, K, W, local, ranks, barrier)
+        extras["large"] = large_line(K, W, local, ranks, barrier)
+        extras.update(run_extras(local))
+        if not a.no_study:
+            from dmm_b200 import workloads as w
+
+            extras["precision_study"] = w.precision_study(
+                n=a.study_n, r=a.study_ratio, seeds=range(a.study_seeds),
+                max_steps=a.study_max_steps)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "clause-updates/s", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": t_max / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": n, "m": m, "per_gpu_instances": 1,
-                       "l2": "flushed (256 MiB write) before every timed step",
-                       "parallelism": f"replicas x{world}", "tuning": inst.tuning},
+            "config": bench_config(world),
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": "clause-updates/s",
                     "h2d_bytes_per_step": h2d / E2E_STEPS, "d2h_bytes_per_step": d2h / E2E_STEPS,
                     "path": f"dmm_instance_create + set_state + {E2E_STEPS} steps + assignment "
                             "readback, pinned host buffers"},
             "gpu_launches": K,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": KERNELS[form_name], "peak_kind": peak_kind,
-                         "algo_bytes_per_launch": algo_bytes},
+            "roofline": roofline(algo_bytes, launch_ms, KERNELS[form_name],
+                                 traffic=profiled_traffic("k_staged_n100k.md"),
+                                 note="traffic: ncu DRAM bytes of one launch of this kernel on "
+                                      "this workload, read from the committed profile summary"),
+            "tuning": inst.tuning, "launch_form": form_name,
             "phase_ms_per_step": {"k_clause": clause_ms / K, "k_var": var_ms / K,
                                   "note": "kernel-per-phase form, L2 flushed"},
             "resident": {"value": resident_value, "unit": "clause-updates/s",
                          "ms_per_step": res_ms / max(1, res_steps),
-                         "note": "CUDA-graph launches, no L2 flush (solver's own mode)"},
+                         "note": "cooperative launches of several steps each (the solver's "
+                                 "own launch path), no L2 flush"},
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
-        if extras is not None:
-            line.update(extras)
+        line.update(extras)
         print(json.dumps(line), flush=True)
     inst.close()
     ranks.close()

@@ -1,8 +1,8 @@
 // Right-hand side of a 3-SAT formula for callers that cannot allocate device memory.
 //
 // Some callers run where cudaMalloc is not available to them: inside a host framework
-// whose caching allocator owns all device memory, in a plug-in that may only touch the
-// buffers it is handed, or between the launches of a stream that is being captured.
+// whose caching allocator owns all device memory (a second allocator would fragment it or
+// fail), or in a plug-in that may only touch the buffers it is handed.
 // dmm_rhs3_f32_noalloc serves them: the caller passes device inputs and outputs, and the
 // intermediate data (per-literal contributions, clause values, the variable->slot CSR and
 // counters) lives in one file-scope __device__ array of fixed size, so the call performs
@@ -11,7 +11,13 @@
 // The array, g_na_scratch, is NA_SCRATCH_BYTES (about 2.1 MB) on every GPU that loads the
 // library, for the life of the process.  It bounds the formula: at most NA_MAX_VARS
 // variables and NA_MAX_CLAUSES clauses of exactly three literals, each variable in at
-// most NA_MAX_OCC literal slots.
+// most NA_MAX_OCC literal slots.  The clause memory rate is the scalar alpha of the
+// parameters (no per-clause alpha).
+//
+// The call validates the formula on the device and reads two counters back (literals out
+// of range, over-long variable lists), waiting for the caller's stream each time, so it
+// blocks the calling thread until the work queued before it and its own checks finish; the
+// right-hand side itself is then queued on the stream without waiting for it.
 //
 // Every call uses the same array and leaves its contents behind; each call clears the
 // parts that must start at zero.  Calls whose work overlaps on the GPU (different streams,
@@ -20,8 +26,7 @@
 //
 // Host code cannot use g_na_scratch's name as a device address.  On its first call on a
 // device, the entry point looks the address up with cudaGetSymbolAddress while that
-// device is current and keeps it for later calls on that device; make that first call
-// before any stream capture begins.
+// device is current and keeps it for later calls on that device.
 //
 // The arithmetic is the production FP32 path's (the same clause and canonical-sum device
 // functions), so the output equals dmm_instance_rhs on an FP32 instance bit for bit.
@@ -63,28 +68,33 @@ __global__ void k_na_clear(NaScratch* s, int n) {
   if (blockIdx.x == 0 && threadIdx.x < 8) s->counters[threadIdx.x] = 0;
 }
 
-// Inclusive scan of vend[0..n) (n <= NA_MAX_VARS) in one block of NA_THREADS threads.
+// Inclusive scan of vend[0..n) (n <= NA_MAX_VARS) in one block of NA_THREADS threads: the
+// block walks the array in chunks of NA_THREADS consecutive entries (coalesced loads and
+// stores), scans each chunk with warp shuffles and carries the running total forward.
 __global__ void k_na_scan(NaScratch* s, int n) {
-  __shared__ int32_t part[NA_THREADS];
-  constexpr int per = NA_MAX_VARS / NA_THREADS;
-  const int base = threadIdx.x * per;
-  int32_t run = 0;
-  for (int i = 0; i < per; i++)
-    if (base + i < n) {
-      run += s->vend[base + i];
-      s->vend[base + i] = run;
-    }
-  part[threadIdx.x] = run;
+  __shared__ int32_t wsum[NA_THREADS / 32];
+  __shared__ int32_t carry;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  for (int o = 1; o < NA_THREADS; o <<= 1) {
-    const int32_t a = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+  for (int base = 0; base < n; base += NA_THREADS) {
+    const int i = base + threadIdx.x;
+    const int32_t v = i < n ? s->vend[i] : 0;
+    int32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
     __syncthreads();
-    part[threadIdx.x] += a;
+    int32_t before = carry;
+    for (int k = 0; k < w; k++) before += wsum[k];
+    if (i < n) s->vend[i] = before + x;
+    __syncthreads();  // every thread has read carry and wsum
+    if (threadIdx.x == NA_THREADS - 1) carry = before + x;
     __syncthreads();
   }
-  const int32_t prefix = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
-  for (int i = 0; i < per; i++)
-    if (base + i < n) s->vend[base + i] += prefix;
 }
 
 // Counts literals outside [-n, n] \ {0} (the caller's buffer is never indexed before this).

@@ -276,18 +276,21 @@ dmm_status dmm_instance_trace_phases(dmm_instance* inst, int32_t nsteps, double*
 
 /* ---- right-hand side without device allocation ----------------------------------------- */
 /* No counterpart in the reference.  For callers that may not allocate device memory (a
- * host framework whose allocator owns the GPU, a plug-in limited to the buffers it is
- * given, work issued between captures): the FP32 right-hand side of a formula whose clauses
- * all have three literals, from DEVICE buffers the caller owns:
+ * host framework whose caching allocator owns the GPU, a plug-in limited to the buffers it
+ * is given): the FP32 right-hand side of a formula whose clauses all have three literals,
+ * from DEVICE buffers the caller owns:
  *   lits  3m signed literals,  x  n + 2m floats (V | Xs | Xl),
  *   dxdt  n + 2m floats out,   loc  one int32 out (clauses with C_m >= 1/2),
- *   p     host parameters (NULL: defaults),  stream  a cudaStream_t (NULL: default stream).
+ *   p     host parameters (NULL: defaults; the scalar alpha, no per-clause alpha),
+ *   stream  a cudaStream_t (NULL: default stream).
  * Intermediates live in one fixed __device__ array (about 2.1 MB per GPU, held until the
  * process exits), so n <= 32768, m <= 65536 and at most 1024 literal slots per variable;
- * larger formulas are rejected with DMM_ERR_ARG.  The first call on a device looks up the
- * array's address (make it before any stream capture).  Calls share the array: calls that
- * overlap on the GPU race and must be serialized by the caller.  Results equal
- * dmm_instance_rhs on an FP32 instance. */
+ * larger formulas are rejected with DMM_ERR_ARG, literals outside [-n, n] or zero with
+ * DMM_ERR_LITERAL.  These checks run on the device and the call waits for the stream twice
+ * to read their counters, so it blocks the calling thread; the right-hand side is then
+ * queued on the stream.  The first call on a device looks up the array's address.  Calls
+ * share the array: calls that overlap on the GPU race and must be serialized by the
+ * caller.  Results equal dmm_instance_rhs on an FP32 instance. */
 dmm_status dmm_rhs3_f32_noalloc(const int32_t* lits, int32_t n, int32_t m, const float* x,
                                 const dmm_params* p, float* dxdt, int32_t* loc, void* stream);
 

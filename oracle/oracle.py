@@ -37,9 +37,15 @@ class RunResult(ctypes.Structure):
     ]
 
 
+# Where the reference sources are read from when the harness is built (DYNEX_REFERENCE_DIR
+# overrides); a machine without them uses the prebuilt _ref/ files as they are.
+REF_DIR = os.environ.get("DYNEX_REFERENCE_DIR", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Builds the oracle (and the reference harness where the reference sources exist)."""
-    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    out = subprocess.run(["make", "-C", HERE, "all", f"REF_DIR={REF_DIR}"], capture_output=True,
+                         text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
@@ -182,21 +188,50 @@ def reference_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+def _load_ref():
+    global _ref_lib
+    if _ref_lib is None:
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_setup.argtypes = [ctypes.c_int, ctypes.c_int, _I32, _I64, _D, ctypes.c_int]
+        lib.ref_xl_max.restype = ctypes.c_double
+        lib.ref_rhs.argtypes = [_D, ctypes.c_double, _D, _I, _D]
+        lib.ref_dostep.argtypes = [_D, _D, ctypes.c_double, _D]
+        lib.ref_run.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, _I, _D, _S8, _S8,
+                                ctypes.POINTER(RunResult)]
+        lib.ref_generate_planted.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_ulonglong, _I32, _I64, _S8]
+        lib.ref_initial_state_uniform.argtypes = [_I32, _I64, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_ulonglong, _D]
+        _ref_lib = lib
+    return _ref_lib
+
+
+def planted_instance(n, m, p0=0.08, p1=0.46, seed=0, init_seed=None):
+    """(lits, clause_off, planted, x0) of the library's planted generator and uniform initial
+    state for these arguments, built by the reference harness library (instance_gen.h) so
+    that the process needs nothing else; x0 is None without init_seed."""
+    lib = _load_ref()
+    lits = np.zeros(3 * int(m), dtype=np.int32)
+    off = np.zeros(int(m) + 1, dtype=np.int64)
+    sigma = np.zeros(int(n), dtype=np.int8)
+    if lib.ref_generate_planted(int(n), int(m), float(p0), float(p1), int(seed) & (2**64 - 1),
+                                _ptr(lits, ctypes.c_int32), _ptr(off, ctypes.c_int64),
+                                _ptr(sigma, ctypes.c_byte)) != 0:
+        raise ValueError("bad generator arguments")
+    x0 = None
+    if init_seed is not None:
+        x0 = np.zeros(int(n) + 2 * int(m), dtype=np.float64)
+        lib.ref_initial_state_uniform(_ptr(lits, ctypes.c_int32), _ptr(off, ctypes.c_int64),
+                                      int(n), int(m), int(init_seed) & (2**64 - 1),
+                                      _ptr(x0, ctypes.c_double))
+    return lits, off, sigma, x0
+
+
 class Reference(_Common):
     """The unmodified reference dynex.cc (per-step harness).  One live instance per process."""
 
     def __init__(self, n, m, lits, coff, params=DEFAULT_PARAMS, xl_max=DEFAULT_XL_MAX):
-        global _ref_lib
-        if _ref_lib is None:
-            lib = ctypes.CDLL(REF_SO)
-            lib.ref_setup.argtypes = [ctypes.c_int, ctypes.c_int, _I32, _I64, _D, ctypes.c_int]
-            lib.ref_xl_max.restype = ctypes.c_double
-            lib.ref_rhs.argtypes = [_D, ctypes.c_double, _D, _I, _D]
-            lib.ref_dostep.argtypes = [_D, _D, ctypes.c_double, _D]
-            lib.ref_run.argtypes = [_D, ctypes.c_int, _D, ctypes.c_int, _I, _D, _S8, _S8,
-                                    ctypes.POINTER(RunResult)]
-            _ref_lib = lib
-        self.lib = _ref_lib
+        self.lib = _load_ref()
         self.n, self.m = int(n), int(m)
         self.lits, self.coff = _as_formula(lits, coff)
         p = np.ascontiguousarray(params, dtype=np.float64)

@@ -23,6 +23,8 @@
 #include DYNEX_REF_SRC
 #undef main
 
+#include "instance_gen.h"
+
 namespace {
 
 int g_ready = 0;
@@ -273,6 +275,25 @@ int ref_run(const double* x0, int max_steps, double* dump, int dump_every, int* 
     res->solve_t = solve_t;
   }
   solved = 0;
+  return 0;
+}
+
+// The seeded planted 3-SAT formula and uniform initial state of the library's generator
+// (instance_gen.h), so that a process timing the reference builds its input without the
+// library.  lits: 3m entries; clause_off: m + 1; sigma (optional): n planted signs;
+// x: n + 2m.
+int ref_generate_planted(int nv, int mc, double p0, double p1, unsigned long long seed,
+                         int* lits, long long* clause_off, signed char* sigma) {
+  if (nv < 3 || mc < 0 || p0 < 0 || p1 < 0 || p0 + p1 > 1.0 || !lits || !clause_off) return -1;
+  oracle_gen::planted(nv, mc, p0, p1, seed, lits, reinterpret_cast<int64_t*>(clause_off),
+                      reinterpret_cast<int8_t*>(sigma));
+  return 0;
+}
+
+int ref_initial_state_uniform(const int* lits, const long long* clause_off, int nv, int mc,
+                              unsigned long long seed, double* x) {
+  if (!lits || !clause_off || !x || nv <= 0 || mc < 0) return -1;
+  oracle_gen::uniform_state(lits, reinterpret_cast<const int64_t*>(clause_off), nv, mc, seed, x);
   return 0;
 }
 

@@ -18,6 +18,24 @@ Outputs, next to this script:
                       the SHA-256 of the `v` assignment.
 
     python tests/golden/make_golden.py --only heuristics   # adds/refreshes that entry only
+    python tests/golden/make_golden.py --only large        # adds/refreshes the entries below
+
+The "large" entries pin the benchmarked sizes (formulas and initial states from the
+library's seeded generator, restated in oracle/instance_gen.h and built here by the
+reference harness library):
+  fixture_n10000.npz  the reference's n = 10000 fixture as arrays (its CLI known answer,
+                      156 steps and T = 13.62 for seed 0, is in known_answers.json)
+  large.c2_bench_fp64     n = 100000, m = 800000, p1 = 0.46 (the bench formula, seed 1,
+                          initial state seed 1001): the reference harness until it solves
+                          (at most 1000 steps), SHA-256 of the FP64 state every 25 steps
+  large.c2_balanced_fp64  n = 100000, m = 800000 with the fixtures' literal split p1 = 0.58
+                          (seed 2, initial state seed 1002), which does not solve within
+                          1000 steps: the reference harness for 1000 steps, hashes every 50
+  large.c2_balanced_fp32  the same formula and state through the oracle's FP32 restatement
+                          (the reference has no FP32 mode), hashes every 50 steps
+  large.c4_fp64 / c4_fp32 n = 1000000, m = 8000000 (seed 3, initial state seed 1003): the
+                          reference harness (FP64) and the oracle (FP32) for 8 steps, a hash
+                          after every step
 """
 from __future__ import annotations
 
@@ -38,7 +56,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import REF_CLI, Reference, build, read_cnf  # noqa: E402
+from oracle.oracle import REF_CLI, Oracle, Reference, build, planted_instance, read_cnf  # noqa: E402
 
 HASH_STEPS = [0, 1, 2, 3, 5, 10, 20, 50, 100, 150, 200]
 
@@ -103,6 +121,54 @@ def heuristics_case() -> dict:
     return out
 
 
+LARGE_CASES = {
+    # name: (n, m, p0, p1, formula seed, initial-state seed, steps, hash every, engine)
+    "c2_bench_fp64": (100_000, 800_000, 0.08, 0.46, 1, 1001, 1000, 25, "reference"),
+    "c2_balanced_fp64": (100_000, 800_000, 0.08, 0.58, 2, 1002, 1000, 50, "reference"),
+    "c2_balanced_fp32": (100_000, 800_000, 0.08, 0.58, 2, 1002, 1000, 50, "oracle_fp32"),
+    "c4_fp64": (1_000_000, 8_000_000, 0.08, 0.46, 3, 1003, 8, 1, "reference"),
+    "c4_fp32": (1_000_000, 8_000_000, 0.08, 0.46, 3, 1003, 8, 1, "oracle_fp32"),
+}
+
+
+def large_case(name: str) -> dict:
+    n, m, p0, p1, seed, init_seed, steps, every, engine = LARGE_CASES[name]
+    lits, off, _, x0 = planted_instance(n, m, p0, p1, seed, init_seed)
+    if engine == "reference":
+        eng = Reference(n, m, lits, off)
+    else:
+        eng = Oracle(n, m, lits, off, precision="fp32")
+    r = eng.run(x0, steps, dump_every=every)
+    hashes = {str(k * every): state_hash(r["dump"][k]) for k in range(len(r["dump"]))
+              if k * every <= r["steps"]}
+    out = {"n": n, "m": m, "p0": p0, "p1": p1, "seed": seed, "init_seed": init_seed,
+           "max_steps": steps, "engine": engine, "steps": r["steps"], "solved": r["solved"],
+           "solve_step": r["solve_step"], "solve_t": r["solve_t"], "t": r["t"],
+           "hashes": hashes,
+           "pre_sha256": hashlib.sha256(r["pre"].astype("<i1").tobytes()).hexdigest()
+           if r["solved"] else None,
+           "post_sha256": hashlib.sha256(r["post"].astype("<i1").tobytes()).hexdigest()
+           if r["solved"] else None,
+           "loc": r["loc"][: min(len(r["loc"]), 64)].tolist()}
+    print(name, out["steps"], out["solved"], out["solve_step"], file=sys.stderr)
+    return out
+
+
+def large_entries(ref_dir: str, answers: dict) -> None:
+    path = os.path.join(ref_dir, "cnf",
+                        "transformed_barthel_n_10000_r_8.000_p0_0.080_instance_001.cnf")
+    n, m, lits, coff = read_cnf(path)
+    np.savez_compressed(os.path.join(HERE, "fixture_n10000.npz"), lits=lits.astype(np.int16),
+                        off=coff.astype(np.int32), planted=planted_of(path))
+    answers.setdefault("large", {})
+    import multiprocessing as mp
+
+    # one process per case: the reference keeps its formula in process globals
+    with mp.get_context("spawn").Pool(len(LARGE_CASES)) as pool:
+        for name, out in zip(LARGE_CASES, pool.map(large_case, list(LARGE_CASES))):
+            answers["large"][name] = out
+
+
 def planted_of(path: str):
     with open(path) as f:
         first = f.readline()
@@ -115,14 +181,17 @@ def planted_of(path: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-dir", default="/root/reference")
-    ap.add_argument("--only", choices=["heuristics"], default=None)
+    ap.add_argument("--only", choices=["heuristics", "large"], default=None)
     a = ap.parse_args()
     build()
-    if a.only == "heuristics":
+    if a.only is not None:
         path = os.path.join(HERE, "known_answers.json")
         with open(path) as f:
             answers = json.load(f)
-        answers["cli_heuristics"] = heuristics_case()
+        if a.only == "heuristics":
+            answers["cli_heuristics"] = heuristics_case()
+        else:
+            large_entries(a.ref_dir, answers)
         with open(path, "w") as f:
             json.dump(answers, f, indent=1)
         return
@@ -160,6 +229,7 @@ def main():
                 np.array(r["v"], dtype="<i4").tobytes()).hexdigest()
             print(name, 0, r["steps"], r["T"], file=sys.stderr)
     answers["cli_heuristics"] = heuristics_case()
+    large_entries(a.ref_dir, answers)
     np.savez_compressed(os.path.join(HERE, "fixtures.npz"), **arrays)
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(answers, f, indent=1)

@@ -35,7 +35,26 @@ def test_roofline_peak_measured_or_fallback(tmp_path, monkeypatch):
 
 
 def test_traffic_from_committed_profile():
-    t = bench.profiled_traffic()
+    t = bench.profiled_traffic("k_staged_n100k.md")
     text = open(os.path.join(ROOT, "profiles", "k_staged_n100k.md")).read()
     assert t is not None and f"traffic_bytes_per_launch: {int(t)}" in text
     assert 1.0 < t / (28 * 800_000 + 8 * 100_000) < 2.0  # DRAM bytes vs algorithmic bytes
+    assert bench.profiled_traffic("no_such_summary.md") is None
+
+
+def test_reference_arm_runs_the_reference_alone_on_the_bench_config():
+    """`bench.py --impl reference` times the unmodified reference integrator on the bench
+    formula and initial state, built without this repository's library, for exactly the
+    steps it reports, and prints this arm's config."""
+    import subprocess
+
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "2", "--warmup", "3", "--procs", "2"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 3
+    assert line["config"] == bench.bench_config(1)
+    assert line["steps_done_per_process"] == [2, 2]
+    assert line["repo_libraries_loaded"] == ["oracle/_ref/libdynex_ref.so"]
+    assert line["cpu_baseline"]["cores"] == 2 and line["e2e"]["value"] == line["value"]

@@ -51,10 +51,37 @@ def test_oracle_matches_reference_harness_hashes(fixtures, known_answers, name):
 
 
 def test_oracle_n10000_known_answer(known_answers):
-    """The largest fixture is not committed; its known answer is checked by the GPU tests
-    against generated data only through the CLI table."""
+    """The reference CLI's answer on its largest fixture (n = 10000, seed 0): step count, T
+    and the reported assignment (SHA-256 of the `v` list)."""
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "fixture_n10000.npz"))
+    lits, off = z["lits"].astype(np.int32), z["off"].astype(np.int64)
+    o = Oracle(10000, len(off) - 1, lits, off)
+    assert o.check(z["planted"]) == 0
     ka = known_answers["cli"]["n10000_seed0"]
-    assert ka["steps"] == 156 and ka["T"] == 13.62
+    r = o.run(o.init_state(0), 400)
+    assert r["solved"] and r["solve_step"] == ka["steps"]
+    assert round(r["solve_t"], 2) == pytest.approx(ka["T"], abs=1e-9)
+    v = np.array([(i + 1) if a > 0 else -(i + 1) for i, a in enumerate(r["post"])], dtype="<i4")
+    assert hashlib.sha256(v.tobytes()).hexdigest() == ka["v_sha256"]
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("p1,seed,init_seed", [(0.46, 1, 1001), (0.58, 2, 1002), (0.5, 9, None)])
+def test_harness_generator_equals_library_generator(p1, seed, init_seed):
+    """The reference harness builds the bench formulas without the library
+    (oracle/instance_gen.h); both must give the same arrays for the same arguments."""
+    import dmm_b200 as dmm
+    from oracle.oracle import planted_instance
+
+    for n, m in ((100, 800), (5000, 21500), (100_000, 800_000)):
+        lits, off, sigma, x0 = planted_instance(n, m, 0.08, p1, seed, init_seed)
+        f, pl = dmm.generate_planted(n, m, 0.08, p1, seed=seed)
+        assert np.array_equal(lits, f.lits) and np.array_equal(off, f.clause_off)
+        assert np.array_equal(sigma, pl)
+        if init_seed is not None:
+            assert np.array_equal(x0, dmm.initial_state_uniform(f, init_seed))
 
 
 @pytest.mark.skipif(not reference_available(), reason="reference harness not built")
