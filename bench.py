@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--study-ratio", type=float, default=8.0,
                     help="clause-to-variable ratio of the study's formula")
     ap.add_argument("--study-max-steps", type=int, default=5000)
+    ap.add_argument("--prior-art-gpu", action="store_true",
+                    help="only time the reference's GPU prior art (dynex.cu) on the bench formula "
+                         "and print its line (run by the default run in a child process)")
     ap.add_argument("--no-study", action="store_true",
                     help="leave the precision study out of the default run")
     return ap.parse_args()
@@ -193,6 +196,7 @@ def peaks() -> tuple[float, str]:
 
 
 KERNELS = {"staged": "k_staged (fused step, staged form)",
+           "staged-multi": "k_staged (fused step, staged form, several tiles per block)",
            "cooperative-single": "k_persist (fused step, single formula)",
            "cooperative": "k_persist (fused step)",
            "two-kernel": "k_clause + k_var", "one-block-per-formula": "k_inst"}
@@ -275,6 +279,39 @@ def cpu_reference(steps: int, warmup: int, procs: int):
     libs = sorted({x for r in res for x in r[2]})
     return N_CLAUSES * done / t, {"procs": procs, "steps_each": [r[0] for r in res],
                                   "timed_s": t, "wall_s": wall, "libraries": libs}
+
+
+def prior_art_gpu(steps: int, warmup: int) -> dict:
+    """The reference's own GPU code (dynex.cu, unmodified, built for sm_100a by
+    oracle/Makefile) on the bench formula and initial state: its FP64 kernels with one thread
+    per clause and CAS-loop atomics, and its host loop that reads loc, energy and each
+    adaptive trial's changed-variable count back every step.  Wall time of `steps` steps
+    (the loop synchronizes at every copy) after `warmup` untimed ones."""
+    from oracle.oracle import GpuPriorArt, planted_instance
+
+    lits, off, _, x0 = planted_instance(N_VARS, N_CLAUSES, P0, P1, INSTANCE_SEED, INIT_SEED)
+    g = GpuPriorArt(N_VARS, N_CLAUSES, lits, off)
+    g.run(x0, warmup)
+    ms, done, loc = g.run(x0, steps)
+    g.close()
+    return {"impl": "dynex.cu (the reference's GPU prior art), FP64", "value": N_CLAUSES * done / (ms / 1e3),
+            "unit": "clause-updates/s", "ms_per_step": ms / max(1, done), "steps": done,
+            "workload": WORKLOAD, "timing": "host wall clock around its synchronous loop"}
+
+
+def prior_art_child(steps: int, warmup: int) -> dict | None:
+    """prior_art_gpu in a child process (its statically linked CUDA runtime stays out of this
+    process); None when the prebuilt library is absent or the run fails."""
+    from oracle.oracle import REF_GPU_SO
+
+    if not os.path.exists(REF_GPU_SO):
+        return None
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--prior-art-gpu", "--steps",
+                        str(steps), "--warmup", str(warmup)], capture_output=True, text=True,
+                       timeout=600)
+    if r.returncode != 0:
+        return {"unavailable": (r.stderr.strip().splitlines() or ["failed"])[-1][:200]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
 
 
 def run_reference_arm(a):
@@ -490,6 +527,9 @@ def main():
     if a.impl == "reference":
         run_reference_arm(a)
         return
+    if a.prior_art_gpu:
+        print(json.dumps(prior_art_gpu(a.steps, max(3, a.warmup))), flush=True)
+        return
     if a.precision_study:
         from dmm_b200 import workloads as w
 
@@ -553,6 +593,9 @@ def main():
     extras = {}
     if rank == 0 and world == 1 and not a.no_extras:
         extras["fp64"] = fp64_line(form, x0, K, W, local, ranks, barrier)
+        pa = prior_art_child(K, W)
+        if pa is not None:
+            extras["prior_art_gpu"] = pa
         extras["large"] = large_line(K, W, local, ranks, barrier)
         extras.update(run_extras(local))
         if not a.no_study:

@@ -191,7 +191,11 @@ class Pack {
   dmm_status capture(int32_t steps);
   dmm_status launch_persist(int32_t nsteps);
   dmm_status launch_inst(int32_t nsteps);
-  dmm_status prepare_xpose(int32_t idx, int TC, int TV, bool* ok);
+  dmm_status prepare_xpose(int32_t idx, int TC, int TV, bool mt, bool* ok);
+  // several-tiles-per-block staged form for a formula too large for one tile per block:
+  // retiles formula idx and builds the tables for the first tiling that fits
+  dmm_status prepare_xpose_mt(int32_t idx, bool* ok);
+  dmm_status set_tiles(int32_t idx, int TC, int TV);
   dmm_status ensure_flush(int64_t bytes);
   const void* persist_fn() const;
   dmm_status enqueue_step(bool rhs_only, void* dv_out);
@@ -238,10 +242,11 @@ class Pack {
     int32_t idx;
     int64_t var0, slot0;
     int32_t n, m, tc, tv, g;
+    bool mt;
     uint64_t serial;
     bool operator==(const XpKey& o) const {
       return idx == o.idx && var0 == o.var0 && slot0 == o.slot0 && n == o.n && m == o.m &&
-             tc == o.tc && tv == o.tv && g == o.g && serial == o.serial;
+             tc == o.tc && tv == o.tv && g == o.g && mt == o.mt && serial == o.serial;
     }
   };
   XpKey xp_key_{};
@@ -252,7 +257,8 @@ class Pack {
          kXpScratch, kXpBufs };
   void* xbuf_[kXpBufs] = {};
   int64_t xbuf_cap_[kXpBufs] = {};
-  int32_t xsv_cap_ = 0, xbk_cap_ = 0, xtv_cap_ = 0, xsmem_ = 0;
+  int32_t xsv_cap_ = 0, xbk_cap_ = 0, xtv_cap_ = 0, xst_cap_ = 0, xsmem_ = 0;
+  bool xp_mt_ = false;  // the staged form runs several tiles per block
   long long* trace_ = nullptr;
   int64_t trace_cap_ = 0;
   bool trace_on_ = false;

@@ -27,6 +27,14 @@
 //
 // Every clause value and every per-variable sum is computed from the same operands in the
 // same order as the plain tile code, so results are identical to it.
+//
+// Several tiles per block (MT): formulas too large for one clause tile and one variable
+// tile per block (the tiles' 16-bit indices and shared memory bound them) are cut into
+// more tiles than blocks; block b takes clause tiles b, b + grid, ... in phase A and
+// variable tiles b, b + grid, ... in phase B, loading each tile's tables when it starts
+// it.  In phase B the bucket overlays the voltage and staging areas of phase A, so a
+// variable tile may hold more contributions than a clause tile stages.  The per-block
+// counts are summed over its tiles before the one update of the step accumulators.
 #pragma once
 
 namespace dmm {
@@ -53,6 +61,24 @@ __host__ __device__ inline XpLayout xp_layout(int sv_cap, int bk_cap, int tv_cap
   L.vend = o; o += xp_align16(4 * (tv_cap + 1));  // tile-local CSR ends of the variable tile
   L.cur = o;  o += xp_align16(4 * tv_cap);        // V of the variable tile
   L.unit = o; o += xp_align16(tv_cap);            // unit pins of the variable tile
+  L.total = o;
+  return L;
+}
+
+// Layout of the several-tiles-per-block form: phase A's voltages (sv_cap) and staging area
+// (st_cap) side by side at L.sv and L.bk; phase B's bucket (bk_cap entries) from L.sv over
+// both; the tables of the current variable tile after the larger of the two.
+__host__ __device__ inline XpLayout xp_layout_mt(int sv_cap, int st_cap, int bk_cap, int tv_cap) {
+  XpLayout L;
+  L.sd = 0;
+  L.sv = 0;
+  L.bk = xp_align16(4 * sv_cap);
+  int o = L.bk + xp_align16(4 * st_cap);
+  if (xp_align16(4 * bk_cap) > o) o = xp_align16(4 * bk_cap);
+  L.src8 = o; o += xp_align16(4 * (bk_cap / 8 + 1));
+  L.vend = o; o += xp_align16(4 * (tv_cap + 1));
+  L.cur = o;  o += xp_align16(4 * tv_cap);
+  L.unit = o; o += xp_align16(tv_cap);
   L.total = o;
   return L;
 }
@@ -123,7 +149,7 @@ __device__ __forceinline__ void load_state4(Group4& q, const float* Xs, const fl
   q.al = acm ? *reinterpret_cast<const float4*>(acm + g) : make_float4(alpha, alpha, alpha, alpha);
 }
 
-template <int G, int NT>
+template <int G, int NT, bool MT>
 __global__ void __launch_bounds__(NT, 1)
     k_staged(PackView<float> P, int nsteps, unsigned int* bar, int* err) {
   using T = float;
@@ -135,10 +161,11 @@ __global__ void __launch_bounds__(NT, 1)
   __shared__ double red[NT / 32];
   __shared__ int cnt[2][NT / 32];
   __shared__ int s_ok;
-  const XpLayout LY = xp_layout(P.xsv_cap, P.xbk_cap, P.xtv_cap);
+  const XpLayout LY = MT ? xp_layout_mt(P.xsv_cap, P.xst_cap, P.xbk_cap, P.xtv_cap)
+                        : xp_layout(P.xsv_cap, P.xbk_cap, P.xtv_cap);
   T* sV = reinterpret_cast<T*>(staged_smem + LY.sv);
   T* stage = reinterpret_cast<T*>(staged_smem + LY.bk);  // phase A
-  T* bucket = stage;                             // phase B
+  T* bucket = MT ? sV : stage;                            // phase B
   int* s_src8 = reinterpret_cast<int*>(staged_smem + LY.src8);
   int* s_vend = reinterpret_cast<int*>(staged_smem + LY.vend);
   T* s_cur = reinterpret_cast<T*>(staged_smem + LY.cur);
@@ -163,21 +190,21 @@ __global__ void __launch_bounds__(NT, 1)
     lc.t = S->t;
     lc.best_t = S->best_t;
     dbeg = dcnt = ubase = ulen = bbeg = blen = 0;
-    if (has_c) {
+    if (!MT && has_c) {
       ctile = P.ctiles[b];
       dbeg = __ldg(P.xdoff + 2 * b);
       dcnt = __ldg(P.xdoff + 2 * b + 1);
       ubase = __ldg(P.xubase + b);
       ulen = __ldg(P.xubase + b + 1) - ubase;
     }
-    if (has_v) {
+    if (!MT && has_v) {
       vtile = P.vtiles[b];
       bbeg = __ldg(P.xboff + b);
       blen = __ldg(P.xboff + b + 1) - bbeg;
     }
   }
   __syncthreads();
-  if (has_v) {
+  if (!MT && has_v) {
     const int32_t* vend = P.vend + I.var0;
     const int jb = vtile.begin > 0 ? __ldg(vend + vtile.begin - 1) : 0;
     for (int g = tid; g < blen / 8; g += NT) s_src8[g] = __ldg(P.xsrc8 + bbeg / 8 + g);
@@ -201,7 +228,20 @@ __global__ void __launch_bounds__(NT, 1)
     trace_stamp(P, s, 1);
 
     // ---- phase A
-    if (has_c) {
+    int unsat = 0, vfail = 0;
+    double e = 0.0;
+    // the block's clause tiles: b, b + grid, ... (one, b, without MT)
+    for (int ct = b; ct < nct; ct += MT ? (int)gridDim.x : nct) {
+      if constexpr (MT) {
+        if (tid == 0) {
+          ctile = P.ctiles[ct];
+          dbeg = __ldg(P.xdoff + 2 * ct);
+          dcnt = __ldg(P.xdoff + 2 * ct + 1);
+          ubase = __ldg(P.xubase + ct);
+          ulen = __ldg(P.xubase + ct + 1) - ubase;
+        }
+        __syncthreads();
+      }
       T* __restrict__ Xs = P.Xs + I.cls0;
       T* __restrict__ Xl = P.Xl + I.cls0;
       T* __restrict__ Cp = P.Cp + I.cls0;
@@ -220,8 +260,6 @@ __global__ void __launch_bounds__(NT, 1)
       cp_async_wait_all();
       __syncthreads();
       trace_stamp(P, s, 2);
-      int unsat = 0, vfail = 0;
-      double e = 0.0;
       auto one = [&](int l0, int l1, int l2, int p0, int p1, int p2, T& xs, T& xl, T cp,
                      T al) -> T {
         if (pending) advance_memory(xs, xl, cp, al, kc);
@@ -307,6 +345,14 @@ __global__ void __launch_bounds__(NT, 1)
       } else if (g_end + tid < c_end) {
         single(g_end + tid);  // fewer than 4 clauses
       }
+      if constexpr (MT) {
+        __syncthreads();  // the staging area is complete
+        float4* __restrict__ dst = reinterpret_cast<float4*>(P.ux + ubase);
+        const float4* src = reinterpret_cast<const float4*>(stage);
+        for (int i = tid; i < ulen / 4; i += NT) dst[i] = src[i];
+        __syncthreads();  // before the next tile reuses the voltage and staging areas
+        continue;
+      }
       unsat = warp_sum_i(unsat);
       vfail = warp_sum_i(vfail);
       if ((tid & 31) == 0) {
@@ -331,6 +377,28 @@ __global__ void __launch_bounds__(NT, 1)
         atomicAdd(&acc->energy, (unsigned long long)et);
       }
     }
+    if constexpr (MT) {
+      if (has_c) {  // the counts of all the block's clause tiles, once
+        unsat = warp_sum_i(unsat);
+        vfail = warp_sum_i(vfail);
+        if ((tid & 31) == 0) {
+          cnt[0][tid >> 5] = unsat;
+          cnt[1][tid >> 5] = vfail;
+        }
+        const double et = block_sum<NT>(e, red) * kEnergyUnitF32;
+        if (tid == 0) {
+          int tu = 0, tv = 0;
+#pragma unroll
+          for (int i = 0; i < NT / 32; i++) {
+            tu += cnt[0][i];
+            tv += cnt[1][i];
+          }
+          if (tu) atomicAdd(&acc->loc, tu);
+          if (tv) atomicAdd(&acc->vfail, tv);
+          atomicAdd(&acc->energy, (unsigned long long)et);
+        }
+      }
+    }
     trace_stamp(P, s, 3);
 
     // ---- barrier 1 (split): the variable tile's voltages load during the wait
@@ -340,9 +408,9 @@ __global__ void __launch_bounds__(NT, 1)
     }
     target += gridDim.x + (s == 0 ? P.barrier_extra : 0);
     T cv = T(0);
-    const int nv = has_v ? vtile.count : 0, v0 = has_v ? vtile.begin : 0;
-    if (has_v) {
-      if (tid < nv) cv = V[v0 + tid];  // V(step) of the tile's variables
+    if (has_v) {  // V(step) of the (first) variable tile's variables
+      const Tile t0 = MT ? P.vtiles[b] : vtile;
+      if (tid < t0.count) cv = V[t0.begin + tid];
     }
     if (tid == 0) {
       int ok = 1;
@@ -376,7 +444,25 @@ __global__ void __launch_bounds__(NT, 1)
     trace_stamp(P, s, 5);
 
     // ---- phase B
-    if (has_v) {
+    int kmax_b = 0;
+    // the block's variable tiles: b, b + grid, ... (one, b, without MT)
+    for (int vt = b; vt < nvt; vt += MT ? (int)gridDim.x : nvt) {
+      if constexpr (MT) {
+        if (tid == 0) {
+          vtile = P.vtiles[vt];
+          bbeg = __ldg(P.xboff + vt);
+          blen = __ldg(P.xboff + vt + 1) - bbeg;
+        }
+        __syncthreads();
+        const int32_t* vend = P.vend + I.var0;
+        const int jb = vtile.begin > 0 ? __ldg(vend + vtile.begin - 1) : 0;
+        for (int g = tid; g < blen / 8; g += NT) s_src8[g] = __ldg(P.xsrc8 + bbeg / 8 + g);
+        for (int i = tid; i <= vtile.count; i += NT)
+          s_vend[i] = i == 0 ? 0 : __ldg(vend + vtile.begin + i - 1) - jb;
+        for (int i = tid; i < vtile.count; i += NT) s_unit[i] = P.unit[I.var0 + vtile.begin + i];
+        __syncthreads();
+      }
+      const int nv = vtile.count, v0 = vtile.begin;
       // the tile's chunks, 4 values per thread and pass: one 16-byte load of a chunk (L2,
       // written by other blocks this step) and four shared stores to the values'
       // variable-major positions
@@ -396,14 +482,17 @@ __global__ void __launch_bounds__(NT, 1)
           if (d3 != kXpPad) bucket[d3] = val.w;
         }
       }
-      if (tid < nv) s_cur[tid] = cv;
-      for (int i = tid + NT; i < nv; i += NT) s_cur[i] = V[v0 + i];
+      if (vt == b) {
+        if (tid < nv) s_cur[tid] = cv;
+        for (int i = tid + NT; i < nv; i += NT) s_cur[i] = V[v0 + i];
+      } else {
+        for (int i = tid; i < nv; i += NT) s_cur[i] = V[v0 + i];
+      }
       __syncthreads();
       trace_stamp(P, s, 6);
       T* __restrict__ nxt = P.cand + (int64_t)((set ^ 1) * kTrials) * P.var_cap + I.var0;
       constexpr int VPP = NT / G;
       const int grp = tid / G, lane = tid % G;
-      int kmax_b = 0;
       for (int vb = 0; vb < nv; vb += VPP) {
         const int i = vb + grp;
         const bool valid = i < nv;
@@ -449,6 +538,9 @@ __global__ void __launch_bounds__(NT, 1)
           kmax_b = max(kmax_b, kv);
         }
       }
+      if constexpr (MT) __syncthreads();  // before the next tile reuses the shared tables
+    }
+    if (has_v) {
       kmax_b = warp_max_i(kmax_b);
       if ((tid & 31) == 0) cnt[0][tid >> 5] = kmax_b;
     }

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -222,6 +223,7 @@ static int persist_threads(dmm_precision prec) {
   return prec == DMM_FP64 ? kPersistThreads64 : kPersistThreads;
 }
 constexpr int kXpSmemMax = 220 * 1024;  // dynamic shared memory of the staged form, at most
+constexpr int kXpMaxTiles = 1 << 14;    // clause or variable tiles of the staged form, at most
 constexpr int kMiscInts = 48;            // misc_d_: 192 bytes
 constexpr int kMiscLaunch = 16;          // misc_d_ index of the per-launch area (byte 64)
 constexpr int kMiscAcc2 = 20;            // misc_d_ index of the StepAcc pair (byte 80)
@@ -937,6 +939,7 @@ void Pack::fill_view(void* vv) const {
   v.xsv_cap = xsv_cap_;
   v.xbk_cap = xbk_cap_;
   v.xtv_cap = xtv_cap_;
+  v.xst_cap = xst_cap_;
   v.barrier_extra = barrier_extra_;
   v.trace = trace_on_ ? trace_ : nullptr;
   v.trace_steps = trace_on_ ? trace_steps_ : 0;
@@ -1023,35 +1026,39 @@ static const void* persist_fn_x(dmm_precision prec, int G) {
   }
 }
 
-// the staged form (FP32, single formula)
-static const void* staged_fn(int G) {
+// the staged form (FP32, single formula); mt: several tiles per block
+template <bool MT>
+static const void* staged_fn_x(int G) {
   switch (G) {
-    case 1: return (const void*)k_staged<1, kStagedThreads>;
-    case 2: return (const void*)k_staged<2, kStagedThreads>;
-    case 4: return (const void*)k_staged<4, kStagedThreads>;
-    case 8: return (const void*)k_staged<8, kStagedThreads>;
-    case 16: return (const void*)k_staged<16, kStagedThreads>;
-    default: return (const void*)k_staged<32, kStagedThreads>;
+    case 1: return (const void*)k_staged<1, kStagedThreads, MT>;
+    case 2: return (const void*)k_staged<2, kStagedThreads, MT>;
+    case 4: return (const void*)k_staged<4, kStagedThreads, MT>;
+    case 8: return (const void*)k_staged<8, kStagedThreads, MT>;
+    case 16: return (const void*)k_staged<16, kStagedThreads, MT>;
+    default: return (const void*)k_staged<32, kStagedThreads, MT>;
   }
+}
+static const void* staged_fn(int G, bool mt) {
+  return mt ? staged_fn_x<true>(G) : staged_fn_x<false>(G);
 }
 
 const void* Pack::persist_fn() const {
-  if (xp_active_) return staged_fn(tun_.var_group);
+  if (xp_active_) return staged_fn(tun_.var_group, xp_mt_);
   if (one_active_) return persist_fn_x<true>(prec_, tun_.var_group);
   return persist_fn_x<false>(prec_, tun_.var_group);
 }
 
 // Tables of the staged form (dmm_xpose.cuh) for formula idx with clause tiles of TC and
-// variable tiles of TV, built on the device (dmm_xprep.cuh).  Leaves *ok false (and the
-// plain tile code in use) when the formula or its tiles do not fit the form's 16-bit
-// indices or shared memory.
-dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
+// variable tiles of TV, built on the device (dmm_xprep.cuh); mt: the several-tiles-per-block
+// form (the tile lists must hold that tiling).  Leaves *ok false (and the plain tile code in
+// use) when the formula or its tiles do not fit the form's 16-bit indices or shared memory.
+dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool mt, bool* ok) {
   *ok = false;
   const InstDesc& I = inst_h_[idx];
   if (prec_ != DMM_FP32 || !I.k3) return DMM_OK;
   // the tables of the same formula at the same place with the same tiles are still valid
   // (only this function writes them, and a live formula's device arrays do not change)
-  const XpKey key{idx, I.var0, I.slot0, I.n, I.m, TC, TV, tun_.var_group, add_serial_[idx]};
+  const XpKey key{idx, I.var0, I.slot0, I.n, I.m, TC, TV, tun_.var_group, mt, add_serial_[idx]};
   if (xp_key_valid_ && key == xp_key_) {
     *ok = true;
     return DMM_OK;
@@ -1059,16 +1066,18 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   xp_key_valid_ = false;
   const int m = I.m, n = I.n, L = I.nslots;
   const int nct = (m + TC - 1) / TC, nvt = (n + TV - 1) / TV;
-  if (nct <= 0 || nvt <= 0 || nct > grid_p_ || nvt > grid_p_ || nvt > kXprepThreads)
-    return DMM_OK;
+  if (nct <= 0 || nvt <= 0) return DMM_OK;
+  if (!mt && (nct > grid_p_ || nvt > grid_p_)) return DMM_OK;
+  if (nct > kXpMaxTiles || nvt > kXpMaxTiles) return DMM_OK;
   const int W = (n + 31) / 32;
-  const int smem_k = (nvt + 2 * W) * 4;
+  const int RW = std::min(W, kXpRangeWords);
+  const int smem_k = (nvt + 2 * RW) * 4;
   if (smem_k > kXpSmemMax) return DMM_OK;
   const int64_t pairs = (int64_t)nct * nvt;
   const int64_t ux_cap = (int64_t)L + 8 * pairs;  // sector padding: < 8 per chunk
-  if (ux_cap > INT32_MAX) return DMM_OK;
-  // scratch: cnt, sb, bt (pairs each), st, dcnt (nct each), out (8)
-  const int64_t scratch_ints = 3 * pairs + 2 * (int64_t)nct + 8;
+  if (ux_cap > INT32_MAX / 2) return DMM_OK;
+  // scratch: cnt, sb, bt (pairs each), st, dcnt (nct each), btot (nvt), out (8)
+  const int64_t scratch_ints = 3 * pairs + 2 * (int64_t)nct + nvt + 8;
   const int64_t bytes[kXpBufs] = {
       ((int64_t)L + 4 * nct) * 4,  // dlist
       2 * (int64_t)nct * 4,        // doff
@@ -1096,7 +1105,8 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
   int* bt = sb + pairs;
   int* st = bt + pairs;
   int* dcnt = st + nct;
-  int* out = dcnt + nct;
+  int* btot = dcnt + nct;
+  int* out = btot + nvt;
   auto* dlist = static_cast<int32_t*>(xbuf_[kXpDlist]);
   auto* doff = static_cast<int32_t*>(xbuf_[kXpDoff]);
   auto* llit = static_cast<int16_t*>(xbuf_[kXpLlit]);
@@ -1116,31 +1126,98 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool* ok) {
     DMM_CUDA(cudaFuncSetAttribute(k_xp_fill<kXprepThreads>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem_k));
   }
-  k_xp_count<kXprepThreads><<<nct, kXprepThreads, smem_k, stream_>>>(lit, L, TC, TV, nvt, W, cnt,
-                                                                     sb, st, dcnt, spos);
+  k_xp_count<kXprepThreads><<<nct, kXprepThreads, smem_k, stream_>>>(lit, L, TC, TV, nvt, n, RW,
+                                                                     cnt, sb, st, dcnt, spos);
   k_xp_scan<kXprepThreads><<<1, kXprepThreads, 0, stream_>>>(nct, nvt, cnt, st, dcnt, ubase,
-                                                             doff, bt, boff, out);
+                                                             doff, bt, boff, btot, out);
   k_xp_fill<kXprepThreads><<<nct, kXprepThreads, smem_k, stream_>>>(
-      lit, upos, vend, L, TC, TV, nct, nvt, W, sb, ubase, doff, bt, boff, dlist, llit, spos, dst,
-      src8);
+      lit, upos, vend, L, TC, TV, nct, nvt, n, RW, sb, ubase, doff, bt, boff, dlist, llit, spos,
+      dst, src8);
   DMM_CUDA(cudaGetLastError());
   int h[8];
   DMM_CUDA(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, stream_));
   DMM_CUDA(cudaStreamSynchronize(stream_));
   if (h[0] != 0) return DMM_OK;
   const int sv_cap = std::max(h[1], 4);
-  const int bk_cap = std::max(h[2], 8);
-  const int smem = xp_layout(sv_cap, bk_cap, TV).total;
+  const int st_cap = std::max(h[6], 8);
+  const int bk_cap = mt ? std::max(h[7], 8) : std::max(h[2], 8);
+  const int smem = mt ? xp_layout_mt(sv_cap, st_cap, bk_cap, TV).total
+                      : xp_layout(sv_cap, bk_cap, TV).total;
   if (smem > kXpSmemMax) return DMM_OK;
-  if (occupancy_blocks(staged_fn(tun_.var_group), kStagedThreads, smem) * sms_ != grid_p_)
+  if (occupancy_blocks(staged_fn(tun_.var_group, mt), kStagedThreads, smem) * sms_ != grid_p_)
     return DMM_OK;
   xsv_cap_ = sv_cap;
+  xst_cap_ = st_cap;
   xbk_cap_ = bk_cap;
   xtv_cap_ = TV;
   xsmem_ = smem;
+  xp_mt_ = mt;
   xp_key_ = key;
   xp_key_valid_ = true;
   *ok = true;
+  return DMM_OK;
+}
+
+// Tile lists of the single live formula idx (the only entries of the tables).
+dmm_status Pack::set_tiles(int32_t idx, int TC, int TV) {
+  InstDesc& I = inst_h_[idx];
+  ctiles_h_.clear();
+  vtiles_h_.clear();
+  I.ctile0 = 0;
+  for (int32_t b = 0; b < I.m; b += TC) ctiles_h_.push_back(Tile{idx, b, std::min(TC, I.m - b), 0});
+  I.nctile = (int32_t)ctiles_h_.size();
+  I.vtile0 = 0;
+  for (int32_t b = 0; b < I.n; b += TV) vtiles_h_.push_back(Tile{idx, b, std::min(TV, I.n - b), 0});
+  I.nvtile = (int32_t)vtiles_h_.size();
+  if ((int64_t)ctiles_h_.size() > ctile_cap_ || (int64_t)vtiles_h_.size() > vtile_cap_) {
+    set_error("tile tables overflow");
+    return DMM_ERR_BUDGET;
+  }
+  return upload_desc(idx);
+}
+
+// The several-tiles-per-block staged form: k_c clause tiles and k_v variable tiles per block
+// (tile counts multiples of the grid, so that every block has the same number).  Candidate
+// tilings whose estimated shared memory fits are ordered by an estimate of their step time
+// (a fixed cost per tile a block visits, plus the bytes of the tiles' variable lists and of
+// the chunk padding at the measured HBM rate); the first one whose tables build and fit is
+// kept.  Leaves *ok false, with the tile lists in an unspecified state, when none fits.
+dmm_status Pack::prepare_xpose_mt(int32_t idx, bool* ok) {
+  *ok = false;
+  const InstDesc& I = inst_h_[idx];
+  if (prec_ != DMM_FP32 || !I.k3) return DMM_OK;
+  const double n = I.n, m = I.m;
+  const int grid = grid_p_;
+  struct Cand {
+    int TC, TV;
+    double cost;
+  };
+  std::vector<Cand> cands;
+  for (int kc = 1; kc <= 64; kc++) {
+    const int TC = (int)(((int64_t)std::ceil(m / (kc * (double)grid)) + 3) & ~int64_t(3));
+    if (TC < kMinClauseTile) break;
+    const double nct = std::ceil(m / TC);
+    const double distinct = n * (1.0 - std::exp(-3.0 * TC / n));
+    for (int kv = 1; kv <= 64; kv++) {
+      const int TV = (int)(((int64_t)std::ceil(n / (kv * (double)grid)) + 3) & ~int64_t(3));
+      if (TV < kMinVarTile) break;
+      const double nvt = std::ceil(n / TV);
+      const double stage = 3.0 * TC + 3.5 * nvt;
+      const double bucket = 3.0 * m / nvt * 1.08 + 3.5 * nct;
+      if (distinct > 30000 || stage > 60000 || bucket > 60000) continue;
+      const double smem = 4.0 * std::max(distinct * 1.03 + stage, bucket) + 0.5 * bucket +
+                          9.0 * TV + 4096;
+      if (smem > 0.97 * kXpSmemMax) continue;
+      const double bytes = 4.0 * distinct * nct + 8.0 * 3.5 * nct * nvt;
+      cands.push_back({TC, TV, 2.0 * (kc + kv) + bytes / 6.0e6});
+    }
+  }
+  std::sort(cands.begin(), cands.end(), [](const Cand& a, const Cand& b) { return a.cost < b.cost; });
+  for (size_t k = 0; k < cands.size() && k < 4; k++) {
+    DMM_TRY(set_tiles(idx, cands[k].TC, cands[k].TV));
+    DMM_TRY(prepare_xpose(idx, cands[k].TC, cands[k].TV, true, ok));
+    if (*ok) return DMM_OK;
+  }
   return DMM_OK;
 }
 
@@ -1232,8 +1309,14 @@ dmm_status Pack::commit_tiles() {
   // one FP32 formula on the cooperative path: two grid barriers per step; with the
   // default layout and tiles, the staged form when it fits
   one_active_ = coop && prec_ == DMM_FP32 && live_list.size() == 1 && small_list.empty();
-  if (one_active_ && tun_.u_layout == 0 && tun_.clause_tile == 0 && tun_.var_tile == 0)
-    DMM_TRY(prepare_xpose(live_list[0], TC, TV, &xp_active_));
+  if (one_active_ && tun_.u_layout == 0 && tun_.clause_tile == 0 && tun_.var_tile == 0) {
+    DMM_TRY(prepare_xpose(live_list[0], TC, TV, false, &xp_active_));
+    // too large for one tile per block: several tiles per block, else the tiles above
+    if (!xp_active_) {
+      DMM_TRY(prepare_xpose_mt(live_list[0], &xp_active_));
+      if (!xp_active_) DMM_TRY(set_tiles(live_list[0], TC, TV));
+    }
+  }
   if (!ctiles_h_.empty())
     DMM_CUDA(cudaMemcpyAsync(ctiles_d_, ctiles_h_.data(), ctiles_h_.size() * sizeof(Tile),
                              cudaMemcpyHostToDevice, stream_));
@@ -1442,7 +1525,8 @@ dmm_status Pack::preload_kernels() {
     fns.push_back((const void*)k_get_state<float>);
     fns.push_back((const void*)k_signs<float>);
     fns.push_back(persist_fn_x<true>(prec_, G));
-    fns.push_back(staged_fn(G));
+    fns.push_back(staged_fn(G, false));
+    fns.push_back(staged_fn(G, true));
     fns.push_back((const void*)k_xp_count<kXprepThreads>);
     fns.push_back((const void*)k_xp_scan<kXprepThreads>);
     fns.push_back((const void*)k_xp_fill<kXprepThreads>);
@@ -1465,7 +1549,7 @@ dmm_status Pack::preload_kernels() {
 int Pack::launch_form() const {
   if (tun_.launch_mode == 1) return 1;
   if (ctiles_h_.empty() && vtiles_h_.empty() && n_small_ > 0) return 5;
-  if (xp_active_) return 4;
+  if (xp_active_) return xp_mt_ ? 6 : 4;
   if (one_active_) return 3;
   return 2;
 }

@@ -193,7 +193,7 @@ class Instance:
         return ms.value
 
     LAUNCH_FORMS = {1: "two-kernel", 2: "cooperative", 3: "cooperative-single",
-                    4: "staged", 5: "one-block-per-formula"}
+                    4: "staged", 5: "one-block-per-formula", 6: "staged-multi"}
 
     @property
     def launch_form(self) -> str:

@@ -241,6 +241,8 @@ dmm_status dmm_instance_assignment(dmm_instance* inst, int8_t* pre, int8_t* post
  *   2  one cooperative kernel for several steps, three grid barriers per step
  *   3  the same for a single FP32 formula: two grid barriers per step
  *   4  the staged single-formula kernel (FP32, 3-literal clauses, tables fit)
+ *   6  the staged kernel with several clause and variable tiles per block (formulas whose
+ *      tiles are too large for one of each per block)
  *   5  one block per formula
  * or a negative dmm_status. */
 int32_t dmm_instance_launch_form(const dmm_instance* inst);

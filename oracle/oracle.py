@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libdynex_ref.so")
 REF_CLI = os.path.join(HERE, "_ref", "dynex_ref")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libdynex_gpu_ref.so")
 
 DEFAULT_PARAMS = (2.5, 20.0, 0.25, 0.05, 0.1, 0.1)  # dynex.cc:132-138
 DEFAULT_XL_MAX = 10000  # dynex.cc:140
@@ -264,6 +265,38 @@ class Reference(_Common):
 
     def run(self, x0, max_steps, dump_every=0):
         return self._run_common(self.lib.ref_run, x0, max_steps, dump_every)
+
+
+class GpuPriorArt:
+    """The reference's GPU prior art (dynex.cu, unmodified, sm_100a) driven by its own host
+    loop with a step cap (ref_gpu_harness.cu).  For timing only: its arithmetic differs from
+    dynex.cc (atomics in arbitrary order, its own step-size rule).  One per process."""
+
+    def __init__(self, n, m, lits, coff, params=DEFAULT_PARAMS, xl_max=DEFAULT_XL_MAX):
+        lib = ctypes.CDLL(REF_GPU_SO)
+        lib.refgpu_setup.argtypes = [ctypes.c_int, ctypes.c_int, _I32, _I64, _D, ctypes.c_int]
+        lib.refgpu_run.argtypes = [_D, ctypes.c_int, _D, _I, _I]
+        self.lib = lib
+        self.n, self.m = int(n), int(m)
+        lits, coff = _as_formula(lits, coff)
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        if lib.refgpu_setup(self.n, self.m, _ptr(lits, ctypes.c_int32), _ptr(coff, ctypes.c_int64),
+                            _ptr(p, ctypes.c_double), int(xl_max)) != 0:
+            raise RuntimeError("reference GPU set-up failed")
+
+    def run(self, x0, max_steps):
+        """(wall ms, steps done, last unsatisfied count) of up to max_steps steps from x0."""
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        ms = ctypes.c_double()
+        steps = ctypes.c_int()
+        loc = ctypes.c_int()
+        if self.lib.refgpu_run(_ptr(x0, ctypes.c_double), int(max_steps), ctypes.byref(ms),
+                               ctypes.byref(steps), ctypes.byref(loc)) != 0:
+            raise RuntimeError("reference GPU run failed")
+        return ms.value, steps.value, loc.value
+
+    def close(self):
+        self.lib.refgpu_teardown()
 
 
 def read_cnf(path):

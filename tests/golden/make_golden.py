@@ -19,6 +19,14 @@ Outputs, next to this script:
 
     python tests/golden/make_golden.py --only heuristics   # adds/refreshes that entry only
     python tests/golden/make_golden.py --only large        # adds/refreshes the entries below
+    python tests/golden/make_golden.py --only replicas     # adds/refreshes cli_replicas
+
+cli_replicas: the reference CLI with three replicas (-w 3, one thread each, dynex.cc:2643-2700:
+replica i > 0 runs alpha / i; with seed 0 replicas 0, 1, 2 start at all 1, 0, -1, otherwise
+from one shared mt19937) on fixtures n = 200 and 500, seeds 0 and 1: for every replica that
+printed its solving right-hand side before the first solution stopped the others, its step
+count and T (which replicas get to print depends on thread timing; each printed pair does
+not).
 
 The "large" entries pin the benchmarked sizes (formulas and initial states from the
 library's seeded generator, restated in oracle/instance_gen.h and built here by the
@@ -131,6 +139,32 @@ LARGE_CASES = {
 }
 
 
+def replicas_case(path: str, seed: int) -> dict:
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, os.path.basename(path))
+        shutil.copy(path, p)
+        out = subprocess.run([REF_CLI, "-i", p, "-l", str(seed), "-w", "3"], capture_output=True,
+                             text=True, timeout=600, cwd=d).stdout
+    text = re.sub(r"\x1b\[[0-9;]*m", "", out.replace("\r", "\n"))
+    got = {}
+    for line in text.splitlines():
+        mm = re.search(r"c \[(\d+)\] [0-9.]+s T=([0-9.]+) GLOBAL=.*\(LOC=0\) \((\d+)\)", line)
+        if mm:
+            got.setdefault(mm.group(1), {"steps": int(mm.group(3)), "T": float(mm.group(2))})
+    return got
+
+
+def replicas_entries(ref_dir: str, answers: dict) -> None:
+    answers["cli_replicas"] = {}
+    for n in (200, 500):
+        path = os.path.join(ref_dir, "cnf",
+                            f"transformed_barthel_n_{n}_r_8.000_p0_0.080_instance_001.cnf")
+        for seed in (0, 1):
+            r = replicas_case(path, seed)
+            answers["cli_replicas"][f"n{n}_seed{seed}"] = r
+            print("replicas", n, seed, r, file=sys.stderr)
+
+
 def large_case(name: str) -> dict:
     n, m, p0, p1, seed, init_seed, steps, every, engine = LARGE_CASES[name]
     lits, off, _, x0 = planted_instance(n, m, p0, p1, seed, init_seed)
@@ -181,7 +215,7 @@ def planted_of(path: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-dir", default="/root/reference")
-    ap.add_argument("--only", choices=["heuristics", "large"], default=None)
+    ap.add_argument("--only", choices=["heuristics", "large", "replicas"], default=None)
     a = ap.parse_args()
     build()
     if a.only is not None:
@@ -190,6 +224,8 @@ def main():
             answers = json.load(f)
         if a.only == "heuristics":
             answers["cli_heuristics"] = heuristics_case()
+        elif a.only == "replicas":
+            replicas_entries(a.ref_dir, answers)
         else:
             large_entries(a.ref_dir, answers)
         with open(path, "w") as f:
@@ -229,6 +265,7 @@ def main():
                 np.array(r["v"], dtype="<i4").tobytes()).hexdigest()
             print(name, 0, r["steps"], r["T"], file=sys.stderr)
     answers["cli_heuristics"] = heuristics_case()
+    replicas_entries(a.ref_dir, answers)
     large_entries(a.ref_dir, answers)
     np.savez_compressed(os.path.join(HERE, "fixtures.npz"), **arrays)
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:

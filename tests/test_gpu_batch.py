@@ -204,11 +204,15 @@ def test_many_small_formulas_auto_mode_equal_alone(fixtures):
 
 
 @pytest.mark.parametrize("n,m,form_want", [(200_000, 840_000, "staged"),
-                                           (300_000, 1_260_000, "cooperative-single")])
+                                           (300_000, 1_260_000, "staged-multi"),
+                                           (300_007, 2_400_013, "staged-multi"),
+                                           (1_000_003, 8_000_009, "staged-multi")])
 def test_staged_kernel_limits(n, m, form_want):
-    """The staged kernel applies while its tile tables fit (16-bit indices, shared memory);
-    beyond that the instance runs the plain single-formula kernel.  Either way the states
-    equal the plain kernel's bit for bit."""
+    """The staged kernel runs one clause tile and one variable tile per block while those
+    fit (16-bit indices, shared memory) and several of each per block beyond that (ragged
+    last tiles in the odd sizes; more than one bitmap range of variables when building the
+    tables above 262,144 variables).  Either way the states equal the plain kernel's bit for
+    bit."""
     form, _ = dmm.generate_planted(n, m, p0=0.08, p1=0.46, seed=n)
     x0 = dmm.initial_state_uniform(form, 5)
     outs = []

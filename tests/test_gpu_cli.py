@@ -19,6 +19,10 @@ def run_cli(args, timeout=300):
     return r.stdout
 
 
+def formula_of(f):
+    return dmm.from_arrays(f["lits"], f["off"], f["n"])
+
+
 def parse(out):
     m = re.search(r"c \[(\d+)\] T=([0-9.]+) SOLUTION FOUND", out)
     steps = int(re.search(r"STEPS = (\d+)", out).group(1))
@@ -208,3 +212,47 @@ def test_cli_alpha_heuristic_with_replicas(tmp_path, known_answers):
         assert out["steps"] == ka["steps"] and out["T"] == pytest.approx(ka["T"], abs=1e-9)
     else:
         assert out["steps"] < ka["steps"]
+
+
+@pytest.mark.parametrize("case", ["n200_seed0", "n200_seed1", "n500_seed0", "n500_seed1"])
+def test_replica_portfolio_matches_oracle_and_reference(tmp_path, fixtures, known_answers, case):
+    """-w 3 (dynex.cc:2643-2700): three replicas, replica i from the reference's initial state
+    for the seed with alpha / i, run together as one FP64 batch.  Every replica's trajectory
+    equals the oracle's for that replica bit for bit (solve step, T, final state); every
+    replica the reference CLI saw solve has the reference's step count and T; and the
+    `dynex -w 3` report names the replica that solves in the fewest steps with its answer."""
+    from oracle.oracle import DEFAULT_PARAMS, Oracle
+
+    name, seed = case.split("_seed")
+    seed = int(seed)
+    f = fixtures[name]
+    form = formula_of(f)
+    b = dmm.Batch.for_formulas([form] * 3, precision="fp64")
+    want = []
+    try:
+        for i in range(3):
+            x0, div = dmm.initial_state_reference(form, seed, i)
+            b.add(form, x0, params=_lib.default_params(alpha=2.5 / div), max_steps=2000)
+            o = Oracle(f["n"], f["m"], f["lits"], f["off"], params=(2.5 / div,) + DEFAULT_PARAMS[1:])
+            want.append(o.run(x0, 2000, dump_every=1))
+        b.run()
+        for i in range(3):
+            got, _ = b.result(i)
+            ref = want[i]
+            assert got.solved == ref["solved"]
+            assert got.solved_step == ref["solve_step"] and got.solved_t == ref["solve_t"]
+            assert np.array_equal(b.state(i)[0], ref["dump"][ref["steps"]])
+    finally:
+        b.close()
+    for rid, ka in known_answers["cli_replicas"][case].items():
+        ref = want[int(rid)]
+        assert ref["solve_step"] == ka["steps"]
+        assert round(ref["solve_t"], 2) == pytest.approx(ka["T"], abs=1e-9)
+    path = str(tmp_path / f"{name}.cnf")
+    dmm.write_cnf(form, path)
+    text = run_cli(["-i", path, "-l", str(seed), "-w", "3"])
+    out = parse(text)
+    best = min(range(3), key=lambda i: (want[i]["solve_step"], i))
+    assert re.search(rf"c \[{best}\] T=[0-9.]+ SOLUTION FOUND", text)
+    assert out["steps"] == want[best]["solve_step"]
+    assert out["T"] == pytest.approx(round(want[best]["solve_t"], 2), abs=1e-9)

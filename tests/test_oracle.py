@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import uniform_init
-from oracle.oracle import Oracle, Reference, reference_available
+from oracle.oracle import DEFAULT_PARAMS, Oracle, Reference, reference_available
 
 FIXTURES = ["n100", "n200", "n500", "n1000"]
 
@@ -84,6 +84,21 @@ def test_harness_generator_equals_library_generator(p1, seed, init_seed):
             assert np.array_equal(x0, dmm.initial_state_uniform(f, init_seed))
 
 
+@pytest.mark.parametrize("case", ["n200_seed0", "n200_seed1", "n500_seed0", "n500_seed1"])
+def test_oracle_replicas_match_reference_cli(fixtures, known_answers, case):
+    """Replica portfolio (-w 3): every replica the reference CLI saw solve, with its initial
+    state and alpha / i (dynex.cc:2643-2700), solves at the same step and T in the oracle."""
+    name, seed = case.split("_seed")
+    f = fixtures[name]
+    for rid, ka in known_answers["cli_replicas"][case].items():
+        i = int(rid)
+        o = Oracle(f["n"], f["m"], f["lits"], f["off"],
+                   params=(2.5 / max(i, 1),) + DEFAULT_PARAMS[1:])
+        r = o.run(o.init_state(int(seed), i), 2000)
+        assert r["solved"] and r["solve_step"] == ka["steps"]
+        assert round(r["solve_t"], 2) == pytest.approx(ka["T"], abs=1e-9)
+
+
 @pytest.mark.skipif(not reference_available(), reason="reference harness not built")
 @pytest.mark.parametrize("name", ["n100", "n200"])
 def test_oracle_bitexact_vs_reference_per_step(fixtures, name):
@@ -159,3 +174,18 @@ def test_oracle_long_occurrence_list_vs_reference():
     b = ref.run(x0, 40, dump_every=1)
     assert np.array_equal(a["dump"], b["dump"])
     assert np.array_equal(a["loc"], b["loc"])
+
+
+def test_gpu_prior_art_harness_is_built():
+    """The reference's GPU code (dynex.cu) compiled for sm_100a with its timing driver: the
+    library loads and exports the driver's entry points (it runs only on a GPU)."""
+    import ctypes
+    import os
+
+    from oracle.oracle import REF_GPU_SO
+
+    if not os.path.exists(REF_GPU_SO):
+        pytest.skip("reference sources absent and no prebuilt library")
+    lib = ctypes.CDLL(REF_GPU_SO)
+    for name in ("refgpu_setup", "refgpu_run", "refgpu_teardown"):
+        assert hasattr(lib, name)
