@@ -116,6 +116,50 @@ __device__ __forceinline__ float f4_at(const float4& v, int i) {
   return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
+// L2 eviction policies for the several-tiles-per-block form, whose per-step working set
+// exceeds the L2: the streamed tables and clause memories are marked evict-first, the
+// staging areas written in phase A and read back in phase B evict-last, so that the
+// staging traffic stays in L2 as far as it fits.
+struct L2Pol {
+  uint64_t first, last;
+};
+__device__ __forceinline__ L2Pol make_l2pol(bool plain) {
+  L2Pol p;
+  if (plain) {  // the same accesses with the default priority
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p.first));
+    p.last = p.first;
+  } else {
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p.first));
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p.last));
+  }
+  return p;
+}
+__device__ __forceinline__ float4 ld_hint4(const float* a, uint64_t pol) {
+  float4 v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_hint4(float* a, float4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a),
+               "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ int2 ld_hint_i2(const void* a, uint64_t pol) {
+  int2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, uint64_t pol) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(sa),
+               "l"(gmem), "l"(pol)
+               : "memory");
+}
+
 // The block's copy of the control state of the formula.
 struct StagedCtrl {
   int done, step, set, kcur, pending, best_loc;
@@ -149,6 +193,25 @@ __device__ __forceinline__ void load_state4(Group4& q, const float* Xs, const fl
   q.al = acm ? *reinterpret_cast<const float4*>(acm + g) : make_float4(alpha, alpha, alpha, alpha);
 }
 
+// The same loads marked evict-first in L2 (several-tiles-per-block form).
+__device__ __forceinline__ void load_words4_hint(Group4& q, const int16_t* ll, const uint16_t* sp,
+                                                 int g, uint64_t pol) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    q.lw[r] = ld_hint_i2(ll + 3 * g + 4 * r, pol);
+    const int2 w = ld_hint_i2(sp + 3 * g + 4 * r, pol);
+    q.qw[r] = make_uint2((unsigned)w.x, (unsigned)w.y);
+  }
+}
+__device__ __forceinline__ void load_state4_hint(Group4& q, const float* Xs, const float* Xl,
+                                                 const float* Cp, const float* acm, float alpha,
+                                                 bool pending, int g, uint64_t pol) {
+  q.xs = ld_hint4(Xs + g, pol);
+  q.xl = ld_hint4(Xl + g, pol);
+  q.cp = pending ? ld_hint4(Cp + g, pol) : make_float4(0.f, 0.f, 0.f, 0.f);
+  q.al = acm ? ld_hint4(acm + g, pol) : make_float4(alpha, alpha, alpha, alpha);
+}
+
 template <int G, int NT, bool MT>
 __global__ void __launch_bounds__(NT, 1)
     k_staged(PackView<float> P, int nsteps, unsigned int* bar, int* err) {
@@ -174,6 +237,8 @@ __global__ void __launch_bounds__(NT, 1)
   const int nct = P.ntiles[0], nvt = P.ntiles[1];
   const bool has_c = b < nct, has_v = b < nvt;
   const int ii = P.live[0];
+  L2Pol pol{0, 0};
+  if constexpr (MT) pol = make_l2pol(P.xl2_plain != 0);
 
   trace_launch(P, 0);
   // ---- launch setup: description, control state, ranges, launch-constant tables
@@ -251,7 +316,10 @@ __global__ void __launch_bounds__(NT, 1)
       // the tile's variable list (padded to 4 entries), then each entry replaced in place
       // by its voltage: two rounds of asynchronous copies with every load in flight
       int* sVi = reinterpret_cast<int*>(sV);
-      for (int q = tid; 4 * q < dcnt; q += NT) cp_async16(sVi + 4 * q, P.xdlist + dbeg + 4 * q);
+      for (int q = tid; 4 * q < dcnt; q += NT) {
+        if constexpr (MT) cp_async16_hint(sVi + 4 * q, P.xdlist + dbeg + 4 * q, pol.first);
+        else cp_async16(sVi + 4 * q, P.xdlist + dbeg + 4 * q);
+      }
       cp_async_wait_all();
       __syncthreads();
       for (int i = tid; i < dcnt; i += NT) cp_async4(sV + i, V + sVi[i]);
@@ -284,9 +352,15 @@ __global__ void __launch_bounds__(NT, 1)
           cc[i] = one(i16_at(q.lw, 3 * i), i16_at(q.lw, 3 * i + 1), i16_at(q.lw, 3 * i + 2),
                       u16_at(q.qw, 3 * i), u16_at(q.qw, 3 * i + 1), u16_at(q.qw, 3 * i + 2), xs[i],
                       xl[i], f4_at(q.cp, i), f4_at(q.al, i));
-        *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
-        *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
-        *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+        if constexpr (MT) {
+          st_hint4(Xs + g, make_float4(xs[0], xs[1], xs[2], xs[3]), pol.first);
+          st_hint4(Xl + g, make_float4(xl[0], xl[1], xl[2], xl[3]), pol.first);
+          st_hint4(Cp + g, make_float4(cc[0], cc[1], cc[2], cc[3]), pol.first);
+        } else {
+          *reinterpret_cast<float4*>(Xs + g) = make_float4(xs[0], xs[1], xs[2], xs[3]);
+          *reinterpret_cast<float4*>(Xl + g) = make_float4(xl[0], xl[1], xl[2], xl[3]);
+          *reinterpret_cast<float4*>(Cp + g) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+        }
       };
       auto single = [&](int c) {
         T xs = Xs[c], xl = Xl[c];
@@ -308,8 +382,13 @@ __global__ void __launch_bounds__(NT, 1)
       const int g_end = pairs ? full_end : full_end + (rem & ~3);
       for (int g = g0; g < g_end; g += 4 * NT) {
         Group4 q;
-        load_words4(q, ll, sp, g);
-        load_state4(q, Xs, Xl, Cp, acm, kc.alpha, pending, g);
+        if constexpr (MT) {
+          load_words4_hint(q, ll, sp, g, pol.first);
+          load_state4_hint(q, Xs, Xl, Cp, acm, kc.alpha, pending, g, pol.first);
+        } else {
+          load_words4(q, ll, sp, g);
+          load_state4(q, Xs, Xl, Cp, acm, kc.alpha, pending, g);
+        }
         group(q, g);
       }
       if (pairs) {
@@ -347,9 +426,8 @@ __global__ void __launch_bounds__(NT, 1)
       }
       if constexpr (MT) {
         __syncthreads();  // the staging area is complete
-        float4* __restrict__ dst = reinterpret_cast<float4*>(P.ux + ubase);
         const float4* src = reinterpret_cast<const float4*>(stage);
-        for (int i = tid; i < ulen / 4; i += NT) dst[i] = src[i];
+        for (int i = tid; i < ulen / 4; i += NT) st_hint4(P.ux + ubase + 4 * i, src[i], pol.last);
         __syncthreads();  // before the next tile reuses the voltage and staging areas
         continue;
       }
@@ -472,9 +550,16 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll 4
         for (int q = tid; q < nb4; q += NT) {
           const int p = 4 * q;
-          const float4 val =
-              __ldcg(reinterpret_cast<const float4*>(P.ux + s_src8[p >> 3] + (p & 7)));
-          const uint2 w = __ldg(xd4 + q);
+          float4 val;
+          uint2 w;
+          if constexpr (MT) {
+            val = ld_hint4(P.ux + s_src8[p >> 3] + (p & 7), pol.first);
+            const int2 wi = ld_hint_i2(xd4 + q, pol.first);
+            w = make_uint2((unsigned)wi.x, (unsigned)wi.y);
+          } else {
+            val = __ldcg(reinterpret_cast<const float4*>(P.ux + s_src8[p >> 3] + (p & 7)));
+            w = __ldg(xd4 + q);
+          }
           const unsigned d0 = w.x & 0xffffu, d1 = w.x >> 16, d2 = w.y & 0xffffu, d3 = w.y >> 16;
           if (d0 != kXpPad) bucket[d0] = val.x;
           if (d1 != kXpPad) bucket[d1] = val.y;

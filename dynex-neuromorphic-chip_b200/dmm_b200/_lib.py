@@ -60,10 +60,10 @@ class Tuning(ctypes.Structure):
     _fields_ = [("clause_tile", ctypes.c_int32), ("var_group", ctypes.c_int32),
                 ("var_tile", ctypes.c_int32), ("steps_per_graph", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("launch_mode", ctypes.c_int32),
-                ("u_layout", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("u_layout", ctypes.c_int32), ("l2_policy", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Cnf(ctypes.Structure):

@@ -114,7 +114,9 @@ typedef struct dmm_tuning {
                                on the tile paths, variable-major in the one-block-per-formula
                                kernel), 1 slot-major (gathered through the CSR), 2 variable-
                                major (scattered through the slot positions)                  */
-  int32_t reserved;
+  int32_t l2_policy;        /* staged form with several tiles per block (launch form 6): 0
+                               default (tables and clause memories marked evict-first in L2,
+                               the phase-A staging areas evict-last), 1 no eviction hints   */
 } dmm_tuning;
 
 /* A DIMACS formula held in host memory (allocated by the library). */
