@@ -160,6 +160,21 @@ __device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, ui
                : "memory");
 }
 
+// Prefetch of the byte range [lo, hi) of `base` into L2 (the bulk prefetch needs a 16-byte
+// aligned start and a size that is a multiple of 16: both ends are rounded down, so the range
+// never reaches past the array), in pieces of 4 KB spread over the lanes of one warp.
+__device__ __forceinline__ void prefetch_l2(const void* base, int64_t lo, int64_t hi, int lane) {
+  lo &= ~int64_t(15);
+  hi &= ~int64_t(15);
+  for (int64_t o = lo + 4096 * (int64_t)lane; o < hi; o += 32 * 4096) {
+    const unsigned sz = (unsigned)(hi - o < 4096 ? hi - o : 4096);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                     static_cast<const char*>(base) + o),
+                 "r"(sz)
+                 : "memory");
+  }
+}
+
 // The block's copy of the control state of the formula.
 struct StagedCtrl {
   int done, step, set, kcur, pending, best_loc;
@@ -306,6 +321,21 @@ __global__ void __launch_bounds__(NT, 1)
           ulen = __ldg(P.xubase + ct + 1) - ubase;
         }
         __syncthreads();
+        // one warp asks L2 for the block's next clause tile (its variable list, local
+        // literals, staging positions and clause memories) while this one is processed
+        const int nt = ct + (int)gridDim.x;
+        if (P.xprefetch && nt < nct && tid < 32) {
+          const Tile tn = P.ctiles[nt];
+          const int db = __ldg(P.xdoff + 2 * nt), dc = __ldg(P.xdoff + 2 * nt + 1);
+          const int64_t c0 = tn.begin, c1 = (int64_t)tn.begin + tn.count;
+          prefetch_l2(P.xdlist, 4 * (int64_t)db, 4 * (int64_t)(db + ((dc + 3) & ~3)), tid);
+          prefetch_l2(P.xllit, 6 * c0, 6 * c1, tid);
+          prefetch_l2(P.xspos, 6 * c0, 6 * c1, tid);
+          prefetch_l2(P.Xs + I.cls0, 4 * c0, 4 * c1, tid);
+          prefetch_l2(P.Xl + I.cls0, 4 * c0, 4 * c1, tid);
+          if (lc.pending) prefetch_l2(P.Cp + I.cls0, 4 * c0, 4 * c1, tid);
+          if (I.has_alpha_cm) prefetch_l2(P.alpha_cm + I.cls0, 4 * c0, 4 * c1, tid);
+        }
       }
       T* __restrict__ Xs = P.Xs + I.cls0;
       T* __restrict__ Xl = P.Xl + I.cls0;

@@ -64,6 +64,21 @@ dmm_status dmm_server_create(const dmm_server_config* cfg, dmm_server** out) {
     return DMM_ERR_ARG;
   *out = nullptr;
   dmm::DeviceScope device_scope(cfg->device);
+  // the arena below is reserved up front: the budget must fit the device's free memory,
+  // with headroom for the per-launch buffers and other users of the device
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    dmm::set_error("server: cannot read the device's free memory");
+    return DMM_ERR_CUDA;
+  }
+  constexpr int64_t kHeadroom = int64_t(1) << 30;
+  if (cfg->budget_bytes > (int64_t)free_b - kHeadroom) {
+    dmm::set_error("server: budget of %lld bytes exceeds the device's free memory (%lld of %lld "
+                   "bytes) less 1 GiB of headroom",
+                   (long long)cfg->budget_bytes, (long long)free_b, (long long)total_b);
+    return DMM_ERR_BUDGET;
+  }
   auto* s = new (std::nothrow) dmm_server();
   if (!s) return DMM_ERR_NOMEM;
   s->cfg = *cfg;

@@ -114,9 +114,11 @@ typedef struct dmm_tuning {
                                on the tile paths, variable-major in the one-block-per-formula
                                kernel), 1 slot-major (gathered through the CSR), 2 variable-
                                major (scattered through the slot positions)                  */
-  int32_t l2_policy;        /* staged form with several tiles per block (launch form 6): 0
-                               default (tables and clause memories marked evict-first in L2,
-                               the phase-A staging areas evict-last), 1 no eviction hints   */
+  int32_t l2_policy;        /* staged form with several tiles per block (launch form 6), two
+                               bits: 0 default (tables and clause memories marked evict-first
+                               in L2, the phase-A staging areas evict-last; each block's next
+                               clause tile prefetched into L2); bit 0 set: no eviction
+                               hints; bit 1 set: no prefetch                                 */
 } dmm_tuning;
 
 /* A DIMACS formula held in host memory (allocated by the library). */
@@ -346,7 +348,9 @@ typedef struct dmm_server dmm_server;
 typedef struct dmm_server_config {
   int32_t precision;        /* dmm_precision                                                 */
   int32_t device;
-  int64_t budget_bytes;     /* device-memory budget for resident instances                   */
+  int64_t budget_bytes;     /* device-memory budget for resident instances, reserved at
+                               creation (DMM_ERR_BUDGET when it exceeds the device's free
+                               memory less 1 GiB)                                            */
   int32_t max_slots;        /* most instances resident at once                               */
   int32_t steps_per_launch; /* steps between admission/retire points                         */
 } dmm_server_config;

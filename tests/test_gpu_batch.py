@@ -101,6 +101,17 @@ def test_server_results_equal_alone(fixtures):
         assert done[k]["finish_s"] >= done[k]["admit_s"] >= done[k]["submit_s"]
 
 
+def test_server_budget_beyond_free_memory_is_refused():
+    """The server reserves its budget when it is created, so a budget larger than the
+    device's free memory is refused up front with DMM_ERR_BUDGET (nothing is allocated)."""
+    import torch
+
+    free, total = torch.cuda.mem_get_info()
+    with pytest.raises(dmm.DmmError) as e:
+        dmm.Server(int(total) + (1 << 30), max_slots=4, precision="fp32")
+    assert e.value.name == "DMM_ERR_BUDGET"
+
+
 def test_server_budget_admission(fixtures):
     f = fixtures["n1000"]
     form = formula(f)
