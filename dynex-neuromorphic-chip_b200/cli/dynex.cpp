@@ -240,6 +240,11 @@ int run_tuner(const Opts& o, const TuneOpts& to, const dmm_cnf* cnf) {
       best[i] = curr[i] = std::min(loc, m);
     }
     dmm_instance_destroy(inst);
+    if (!q) {  // the reference's line after its initial objective (dynex.cc:1717-1722)
+      std::printf("c [TUNE] E: ");
+      for (int i = 0; i < R; i++) std::printf("[%.2f]", best[i]);
+      std::printf("\n");
+    }
   }
   const std::string tuning_file = o.input + ".tuning.txt";
   if (FILE* f = std::fopen(tuning_file.c_str(), "w")) {  // dynex.cc:2719-2726

@@ -120,7 +120,8 @@ struct PackView {
   int32_t xsv_cap, xbk_cap, xtv_cap;  // shared-memory capacities (entries)
   int32_t xst_cap;          // staging-area capacity of the several-tiles-per-block form
   int32_t xl2_plain;        // that form without L2 eviction hints
-  int32_t xprefetch;        // that form prefetching each block's next clause tile into L2
+  int32_t xprefetch;        // that form prefetching each block's next clause tile into L2 (off
+                            // by default: measured slower)
   // phase trace of the cooperative kernel (null when off): trace[(s * kTraceK + k) * grid +
   // block] = %globaltimer at step s's point k: 0 start, 1 clause tile loaded, 2 voltages
   // gathered, 3 phase A done, 4 past barrier 1, 5 variable tile loaded, 6 bucket filled,

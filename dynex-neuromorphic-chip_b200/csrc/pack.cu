@@ -369,7 +369,7 @@ dmm_status Pack::set_tuning(const dmm_tuning* t) {
     return DMM_ERR_ARG;
   }
   if (n.l2_policy < 0 || n.l2_policy > 3) {
-    set_error("l2_policy must be 0..3 (bit 0: no eviction hints, bit 1: no L2 prefetch)");
+    set_error("l2_policy must be 0..3 (bit 0: no eviction hints, bit 1: L2 prefetch)");
     return DMM_ERR_ARG;
   }
   if (n.u_layout < 0 || n.u_layout > 2) {
@@ -945,7 +945,7 @@ void Pack::fill_view(void* vv) const {
   v.xtv_cap = xtv_cap_;
   v.xst_cap = xst_cap_;
   v.xl2_plain = tun_.l2_policy & 1;
-  v.xprefetch = !(tun_.l2_policy & 2);
+  v.xprefetch = (tun_.l2_policy & 2) != 0;
   v.barrier_extra = barrier_extra_;
   v.trace = trace_on_ ? trace_ : nullptr;
   v.trace_steps = trace_on_ ? trace_steps_ : 0;

@@ -116,9 +116,10 @@ typedef struct dmm_tuning {
                                major (scattered through the slot positions)                  */
   int32_t l2_policy;        /* staged form with several tiles per block (launch form 6), two
                                bits: 0 default (tables and clause memories marked evict-first
-                               in L2, the phase-A staging areas evict-last; each block's next
-                               clause tile prefetched into L2); bit 0 set: no eviction
-                               hints; bit 1 set: no prefetch                                 */
+                               in L2, the phase-A staging areas evict-last); bit 0 set: no
+                               eviction hints; bit 1 set: one warp per block also prefetches
+                               the block's next clause tile into L2 (measured slower: 71.5
+                               vs 65.8 us per step at n = 300k)                             */
 } dmm_tuning;
 
 /* A DIMACS formula held in host memory (allocated by the library). */

@@ -20,6 +20,15 @@ Outputs, next to this script:
     python tests/golden/make_golden.py --only heuristics   # adds/refreshes that entry only
     python tests/golden/make_golden.py --only large        # adds/refreshes the entries below
     python tests/golden/make_golden.py --only replicas     # adds/refreshes cli_replicas
+    python tests/golden/make_golden.py --only tuner        # adds/refreshes cli_tuner
+
+cli_tuner: the reference CLI's parameter tuner (-t 1) on fixtures n = 1000 (seed 1, three
+replicas) and n = 500 (seed 2, two replicas): the initial objective of every replica, the
+`c [TUNE] E:` line (dynex.cc:1711-1722), which the reference computes with one Euler step
+through odeint's integrate_n_steps (implemented by oracle/boost_stub from Boost.Odeint's
+documented behaviour).  The tuner's later iterations run until a wall-clock limit
+(dynex.cc's default integrator ignores maxsteps), so only this first objective is
+deterministic.
 
 cli_replicas: the reference CLI with three replicas (-w 3, one thread each, dynex.cc:2643-2700:
 replica i > 0 runs alpha / i; with seed 0 replicas 0, 1, 2 start at all 1, 0, -1, otherwise
@@ -165,6 +174,28 @@ def replicas_entries(ref_dir: str, answers: dict) -> None:
             print("replicas", n, seed, r, file=sys.stderr)
 
 
+def tuner_case(path: str, seed: int, replicas: int) -> list:
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, os.path.basename(path))
+        shutil.copy(path, p)
+        out = subprocess.run([REF_CLI, "-i", p, "-l", str(seed), "-w", str(replicas), "-t", "1",
+                              "-s", "1", "-u", "1"], capture_output=True, text=True, timeout=600,
+                             cwd=d).stdout
+    text = re.sub(r"\x1b\[[0-9;]*m", "", out.replace("\r", "\n"))
+    mm = re.search(r"c \[TUNE\] E: ((?:\[[0-9.]+\])+)", text)
+    return [float(v) for v in re.findall(r"\[([0-9.]+)\]", mm.group(1))]
+
+
+def tuner_entries(ref_dir: str, answers: dict) -> None:
+    answers["cli_tuner"] = {}
+    for n, seed, reps in ((1000, 1, 3), (500, 2, 2)):
+        path = os.path.join(ref_dir, "cnf",
+                            f"transformed_barthel_n_{n}_r_8.000_p0_0.080_instance_001.cnf")
+        e = tuner_case(path, seed, reps)
+        answers["cli_tuner"][f"n{n}_seed{seed}_w{reps}"] = {"initial_objective": e}
+        print("tuner", n, seed, reps, e, file=sys.stderr)
+
+
 def large_case(name: str) -> dict:
     n, m, p0, p1, seed, init_seed, steps, every, engine = LARGE_CASES[name]
     lits, off, _, x0 = planted_instance(n, m, p0, p1, seed, init_seed)
@@ -215,7 +246,7 @@ def planted_of(path: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-dir", default="/root/reference")
-    ap.add_argument("--only", choices=["heuristics", "large", "replicas"], default=None)
+    ap.add_argument("--only", choices=["heuristics", "large", "replicas", "tuner"], default=None)
     a = ap.parse_args()
     build()
     if a.only is not None:
@@ -226,6 +257,8 @@ def main():
             answers["cli_heuristics"] = heuristics_case()
         elif a.only == "replicas":
             replicas_entries(a.ref_dir, answers)
+        elif a.only == "tuner":
+            tuner_entries(a.ref_dir, answers)
         else:
             large_entries(a.ref_dir, answers)
         with open(path, "w") as f:
@@ -266,6 +299,7 @@ def main():
             print(name, 0, r["steps"], r["T"], file=sys.stderr)
     answers["cli_heuristics"] = heuristics_case()
     replicas_entries(a.ref_dir, answers)
+    tuner_entries(a.ref_dir, answers)
     large_entries(a.ref_dir, answers)
     np.savez_compressed(os.path.join(HERE, "fixtures.npz"), **arrays)
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:

@@ -256,3 +256,19 @@ def test_replica_portfolio_matches_oracle_and_reference(tmp_path, fixtures, know
     assert re.search(rf"c \[{best}\] T=[0-9.]+ SOLUTION FOUND", text)
     assert out["steps"] == want[best]["solve_step"]
     assert out["T"] == pytest.approx(round(want[best]["solve_t"], 2), abs=1e-9)
+
+
+@pytest.mark.parametrize("case", ["n1000_seed1_w3", "n500_seed2_w2"])
+def test_cli_tuner_initial_objective_matches_reference(tmp_path, fixtures, known_answers, case):
+    """`dynex -t 1`: the tuner's initial objective of every replica (the `c [TUNE] E:` line)
+    equals the reference tuner's, which takes one Euler step through odeint
+    (dynex.cc:1711-1722); its later iterations run to a wall-clock limit in the reference,
+    so only this objective is compared."""
+    name, seed, reps = case.split("_")
+    f = fixtures[name]
+    path = str(tmp_path / f"{name}.cnf")
+    dmm.write_cnf(formula_of(f), path)
+    text = run_cli(["-i", path, "-l", seed[4:], "-w", reps[1:], "-t", "1", "-s", "1", "-z", "20"])
+    m = re.search(r"c \[TUNE\] E: ((?:\[[0-9.]+\])+)", text)
+    got = [float(v) for v in re.findall(r"\[([0-9.]+)\]", m.group(1))]
+    assert got == known_answers["cli_tuner"][case]["initial_objective"]

@@ -99,6 +99,18 @@ def test_oracle_replicas_match_reference_cli(fixtures, known_answers, case):
         assert round(r["solve_t"], 2) == pytest.approx(ka["T"], abs=1e-9)
 
 
+@pytest.mark.parametrize("case", ["n1000_seed1_w3", "n500_seed2_w2"])
+def test_oracle_tuner_initial_objective_matches_reference(fixtures, known_answers, case):
+    """The reference tuner's initial objective (`-t 1`, one Euler step through odeint,
+    dynex.cc:1711-1722) of every replica is the unsatisfied count of its initial state."""
+    name, seed, reps = case.split("_")
+    f = fixtures[name]
+    o = Oracle(f["n"], f["m"], f["lits"], f["off"])
+    want = known_answers["cli_tuner"][case]["initial_objective"]
+    got = [float(o.rhs(o.init_state(int(seed[4:]), i))[1]) for i in range(int(reps[1:]))]
+    assert got == want
+
+
 @pytest.mark.skipif(not reference_available(), reason="reference harness not built")
 @pytest.mark.parametrize("name", ["n100", "n200"])
 def test_oracle_bitexact_vs_reference_per_step(fixtures, name):
