@@ -131,6 +131,22 @@ def run_extras(device: int) -> dict:
                   "p50_tts_s": sp["p50_tts_s"], "p99_tts_s": sp["p99_tts_s"],
                   "path": "same arrivals, one request at a time"},
     }
+    # formulas of the bench's size batched: 64 planted 3-SAT formulas at n = 100,000 in one
+    # pack (the tile kernels, all formulas stepping together) against the same formulas one
+    # at a time on the plain path (the staged kernel, create + solve each)
+    big = w.make_items(64, 100_000, 100_000, ratios=(8.0,), seed=4)
+    bl = w.run_batched(big, max_steps=1000, device=device)
+    pl = w.run_plain(big, max_steps=1000, device=device)
+    assert bl["steps"] == pl["steps"], "per-formula results differ between paths"
+    batched_large = {
+        "workload": "64 planted 3-SAT formulas, n=100000, r=8, p0=0.08, FP32, step cap 1000",
+        "solved": bl["solved"], "solves_per_s_incl_setup": bl["solves_per_s"],
+        "solves_per_s_run": bl["solves_per_s_run"], "setup_s": bl["setup_s"],
+        "clause_updates_per_s": bl["clause_updates_per_s"], "device_ms": bl["device_ms"],
+        "plain": {"solved": pl["solved"], "solves_per_s": pl["solves_per_s"],
+                  "clause_updates_per_s": pl["clause_updates_per_s"]},
+        "solves_ratio_vs_plain": bl["solves_per_s"] / max(pl["solves_per_s"], 1e-9),
+    }
     # the literal-agreement split of the bench (0.08 / 0.46 / 0.46, as the benchmark states it)
     # against the split of the reference's own fixtures (0.08 / 0.58 / 0.34, Barthel's
     # balanced ensemble): same size, same seeds, each ensemble solved as one batch
@@ -147,7 +163,8 @@ def run_extras(device: int) -> dict:
     ensembles = {"workload": "64 planted 3-SAT formulas per ensemble, n=10000, r=8, FP32, "
                              "initial state V~U[-1,1], Xs~U[0,1], Xl=1, step cap 5000",
                  "ensembles": ens}
-    return {"batched": batched, "served": served, "ensembles": ensembles}
+    return {"batched": batched, "batched_large": batched_large, "served": served,
+            "ensembles": ensembles}
 
 
 # ---- helpers ------------------------------------------------------------------------------
