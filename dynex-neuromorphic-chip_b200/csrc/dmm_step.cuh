@@ -93,10 +93,15 @@ struct TileSmem {
 };
 
 // Loads tile `ti` and, when its instance differs from the cached one, the instance
-// description and control snapshot.  Block-wide.
+// description and control snapshot.  Block-wide.  The leading barrier keeps thread 0 from
+// overwriting the previous tile's state while other warps still read it: a tile of a
+// finished formula returns from the tile code at once, with no block barrier of its own, so
+// without it a warp could take the next tile's state for the previous tile and the block's
+// barriers would fall out of step.
 template <class T, int NT>
 __device__ __forceinline__ void load_tile(TileSmem<NT>& sm, const PackView<T>& P, const Tile* tiles,
                                           int ti) {
+  __syncthreads();
   if (threadIdx.x == 0) {
     sm.tile = tiles[ti];
     const int ii = sm.tile.inst;
@@ -619,6 +624,7 @@ struct LocalSnap {
 template <int NT>
 __device__ __forceinline__ void load_tile_one(TileSmem<NT>& sm, const LocalSnap& ls,
                                               const Tile* tiles, int ti) {
+  __syncthreads();  // as in load_tile: the previous tile's state is no longer read
   if (threadIdx.x == 0) {
     sm.tile = tiles[ti];
     sm.snap.done = ls.done;

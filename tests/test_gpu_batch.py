@@ -287,3 +287,30 @@ def test_staged_clause_rounds_with_ragged_tiles(m):
         for r in range(1, 3):
             inst.step(2)
             assert np.array_equal(inst.get_state()[0], ref["dump"][r])
+
+
+def test_cooperative_batch_with_formulas_finishing_at_different_steps():
+    """Many formulas on the cooperative multi-formula kernel, solving at different steps: the
+    tiles of formulas that already finished are skipped while the others keep stepping
+    (the pattern that once let a block's warps fall out of step).  Every formula's result
+    and final state equal its run alone."""
+    forms = [dmm.generate_planted(10_000, 80_000, 0.08, 0.46, seed=500 + k)[0] for k in range(48)]
+    x0s = [dmm.initial_state_uniform(f, 900 + k) for k, f in enumerate(forms)]
+    b = dmm.Batch.for_formulas(forms, precision="fp32")
+    try:
+        b.set_tuning(launch_mode=2)
+        for f, x0 in zip(forms, x0s):
+            b.add(f, x0, max_steps=400)
+        b.run()
+        steps = set()
+        for k, (f, x0) in enumerate(zip(forms, x0s)):
+            got, post_b = b.result(k)
+            want, post_a, x_a = alone(f, x0, "fp32", 400)
+            assert (got.status, got.steps, got.solved_step, got.t, got.loc) == (
+                want.status, want.steps, want.solved_step, want.t, want.loc), k
+            assert np.array_equal(b.state(k)[0], x_a), k
+            assert np.array_equal(post_b, post_a), k
+            steps.add(got.steps)
+        assert len(steps) > 10  # the formulas finish at many different steps
+    finally:
+        b.close()
