@@ -330,6 +330,86 @@ __device__ __noinline__ double sorted_sum_select(const double* u,
   return acc;
 }
 
+// Sorts the N values of one thread ascending in registers: Batcher's odd-even merge sort
+// (191 compare-exchanges for N = 32), every index a compile-time constant once unrolled.
+// Equal values may leave in either order; the left-to-right sum that follows does not
+// depend on it (equal values are interchangeable, and a partial sum that starts at +0.0
+// never becomes -0.0, so the sign of a zero changes no sum either).
+template <int N>
+__device__ __forceinline__ void sort_net(double (&a)[N]) {
+  // merge of sorted runs of p into runs of 2p, at distance k: element i meets i + k when
+  // both lie in the same run of 2p and i - (k mod p) falls in the lower half of a block of 2k
+#pragma unroll
+  for (int p = 1; p < N; p <<= 1) {
+#pragma unroll
+    for (int k = p; k >= 1; k >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        const int j = k % p;
+        if (i >= j && (i - j) % (2 * k) < k && i + k < N && i / (2 * p) == (i + k) / (2 * p)) {
+          const double x = a[i], y = a[i + k];
+          const bool sw = y < x;
+          a[i] = sw ? y : x;
+          a[i + k] = sw ? x : y;
+        }
+      }
+    }
+  }
+}
+
+// Lists longer than one thread's network that a block queues for its second pass.
+constexpr int kLongQueue = 512;
+
+// Several lists per warp, SEG lanes and RQ registers per list (entry e = lane-in-segment +
+// SEG r, +inf beyond the list): one bitonic network sorts every segment's SEG * RQ entries
+// at once, then each segment adds its d smallest left to right (d per segment; the result
+// is valid in every lane of the segment).
+template <int SEG, int RQ>
+__device__ __forceinline__ double seg_sort_sum(double (&a)[RQ], int d, int lane) {
+  const int seg = lane / SEG, sl = lane % SEG;
+#pragma unroll
+  for (int k = 2; k <= SEG * RQ; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= SEG) {  // partner in another register of the same lane
+        const int jr = j / SEG;
+#pragma unroll
+        for (int r = 0; r < RQ; r++) {
+          const int r2 = r ^ jr;
+          if (r2 > r) {
+            const bool up = ((sl + SEG * r) & k) == 0;
+            const double x = a[r], y = a[r2];
+            const bool sw = up ? (y < x) : (x < y);
+            a[r] = sw ? y : x;
+            a[r2] = sw ? x : y;
+          }
+        }
+      } else {  // partner lane sl ^ j of the same segment
+#pragma unroll
+        for (int r = 0; r < RQ; r++) {
+          const int e = sl + SEG * r;
+          const double o = __shfl_xor_sync(0xffffffffu, a[r], j);
+          const bool up = (e & k) == 0;
+          const bool lower = (e & j) == 0;
+          const double mn = (o < a[r]) ? o : a[r];
+          const double mx = (o < a[r]) ? a[r] : o;
+          a[r] = (lower == up) ? mn : mx;
+        }
+      }
+    }
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int r = 0; r < RQ; r++) {
+#pragma unroll
+    for (int l = 0; l < SEG; l++) {
+      const double x = __shfl_sync(0xffffffffu, a[r], seg * SEG + l);
+      if (SEG * r + l < d) acc = __dadd_rn(acc, x);
+    }
+  }
+  return acc;
+}
+
 template <bool DIRECT = false, class Idx = int32_t>
 __device__ __forceinline__ double sorted_sum(const double* u,
                                              const Idx* __restrict__ vs, int d, int lane) {

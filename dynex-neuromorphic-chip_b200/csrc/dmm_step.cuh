@@ -87,7 +87,7 @@ struct TileSmem {
   StepAcc* acc;  // step accumulators (single-formula cooperative form), else null
   int ti;
   int flag;
-  int vnext;  // next 4-variable group of the sorted sums (reset by the tile loaders)
+  int vnext;  // next 32-variable group of the sorted sums (reset by the tile loaders)
   double red[NT / 32];
   int cnt[2][NT / 32];
 };
@@ -313,25 +313,29 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
     }
   };
   if constexpr (SORTED) {
-    // FP64 reference sums: four variables per warp, eight lanes each holding four entries
-    // (entry e = lane-in-segment + 8 r); one bitonic network sorts the four lists at once
-    // and the ascending left-to-right sum takes one shuffle per entry position for all four.
-    // Lists longer than 32 take the warp-wide sum afterwards.  Warps take the groups from a
-    // shared counter: the long lists make groups uneven, and each variable's sum is
-    // computed by one warp alone, so the assignment does not change any result.
+    // FP64 reference sums, one thread per variable: a lane loads its variable's list (up to
+    // 32 entries, +inf beyond its length) into registers, sorts it with a fixed network and
+    // adds it left to right, so a warp keeps the loads of 32 lists in flight and needs no
+    // shuffles.  Lists longer than 32 are queued for the block and summed afterwards, four
+    // per warp.  Warps take their groups from shared counters: each variable's sum is
+    // computed by one thread, one 8-lane segment or one warp alone, so the assignment does
+    // not change any result.
     static_assert(G == 32, "the sorted sum is organized per warp");
-    constexpr int SEG = 8, NV = 32 / SEG, RR = 4;
+    constexpr int R = 32;
+    __shared__ int s_nlong, s_lnext;          // queued long lists; next queue group
+    __shared__ int32_t s_long[kLongQueue];
+    if (threadIdx.x == 0) s_nlong = s_lnext = 0;
+    __syncthreads();
     const double* ud = reinterpret_cast<const double*>(u);
     const double pinf = inf_val<double>();
-    const int seg = lane / SEG, sl = lane % SEG;
     (void)VPP;
     (void)grp;
     for (;;) {
       int gi = 0;
       if (lane == 0) gi = atomicAdd(&sm.vnext, 1);
-      const int vb = sm.tile.begin + NV * __shfl_sync(0xffffffffu, gi, 0);
+      const int vb = sm.tile.begin + 32 * __shfl_sync(0xffffffffu, gi, 0);
       if (vb >= v_end) break;
-      const int v = vb + seg;
+      const int v = vb + lane;
       const bool valid = v < v_end;
       int s0 = 0, d = 0;
       if (valid) {
@@ -339,59 +343,84 @@ __device__ void var_tile(const PackView<T>& P, TileSmem<NT>& sm, double* __restr
         s0 = v > 0 ? __ldg(vend + v - 1) : 0;
         d = s1 - s0;
       }
-      const bool small = valid && d <= SEG * RR;
-      double a[RR];
+      const bool small = valid && d <= R;
+      const int ds = small ? d : 0;
+      // A variable-major list is read with 16-byte loads from the even position at or below
+      // s0 (the instance's arrays start 16-byte aligned and u ends with padding, so the
+      // words past the list stay in the allocation); entry r is word entry (s0 & 1) + r.
+      double a[R];
+      if (P.upos) {  // variable-major contributions: the list itself, two per load
+        const int off = s0 & 1;
+        const double2* w2 = reinterpret_cast<const double2*>(ud + (s0 - off));
+        const int nw = (off + ds + 1) >> 1;
+        double2 w[R / 2 + 1];
 #pragma unroll
-      for (int r = 0; r < RR; r++) {
-        const int e = sl + SEG * r;
-        a[r] = (small && e < d) ? (P.upos ? ud[s0 + e] : ud[__ldg(vsl + s0 + e)]) : pinf;
-      }
+        for (int j = 0; j < R / 2 + 1; j++) w[j] = j < nw ? w2[j] : make_double2(pinf, pinf);
 #pragma unroll
-      for (int k = 2; k <= SEG * RR; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          if (j >= SEG) {  // partner in another register of the same lane
-            const int jr = j / SEG;
-#pragma unroll
-            for (int r = 0; r < RR; r++) {
-              const int r2 = r ^ jr;
-              if (r2 > r) {
-                const bool up = ((sl + SEG * r) & k) == 0;
-                const double x = a[r], y = a[r2];
-                const bool sw = up ? (y < x) : (x < y);
-                a[r] = sw ? y : x;
-                a[r2] = sw ? x : y;
-              }
-            }
-          } else {  // partner lane sl ^ j of the same segment
-#pragma unroll
-            for (int r = 0; r < RR; r++) {
-              const int e = sl + SEG * r;
-              const double o = __shfl_xor_sync(0xffffffffu, a[r], j);
-              const bool up = (e & k) == 0;
-              const bool lower = (e & j) == 0;
-              const double mn = (o < a[r]) ? o : a[r];
-              const double mx = (o < a[r]) ? a[r] : o;
-              a[r] = (lower == up) ? mn : mx;
-            }
-          }
+        for (int r = 0; r < R; r++) {
+          const double e0 = (r & 1) ? w[r >> 1].y : w[r >> 1].x;        // offset 0
+          const double e1 = (r & 1) ? w[(r + 1) >> 1].x : w[r >> 1].y;  // offset 1
+          a[r] = r < ds ? (off ? e1 : e0) : pinf;
         }
+      } else {  // slot-major contributions: gathers through the slot list
+        int q[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) q[r] = r < ds ? __ldg(vsl + s0 + r) : 0;
+#pragma unroll
+        for (int r = 0; r < R; r++) a[r] = r < ds ? ud[q[r]] : pinf;
       }
+      sort_net<R>(a);
       double acc = 0.0;
 #pragma unroll
-      for (int r = 0; r < RR; r++) {
-#pragma unroll
-        for (int l = 0; l < SEG; l++) {
-          const double x = __shfl_sync(0xffffffffu, a[r], seg * SEG + l);
-          if (SEG * r + l < d) acc = __dadd_rn(acc, x);
-        }
+      for (int r = 0; r < R; r++)
+        if (r < ds) acc = __dadd_rn(acc, a[r]);
+      if (small) finish(v, T(acc));
+      // longer lists wait in the block's queue (the ones past its end are summed here)
+      int qs = kLongQueue;
+      if (valid && !small) qs = atomicAdd(&s_nlong, 1);
+      unsigned over = __ballot_sync(0xffffffffu, valid && !small && qs >= kLongQueue);
+      if (valid && !small && qs < kLongQueue) s_long[qs] = v;
+      while (over) {  // warp-uniform
+        const int vl = vb + __ffs(over) - 1;
+        over &= over - 1;
+        const int e1 = __ldg(vend + vl), e0 = vl > 0 ? __ldg(vend + vl - 1) : 0;
+        const double dv = P.upos ? sorted_sum<true, int32_t>(ud + e0, nullptr, e1 - e0, lane)
+                                 : sorted_sum<false>(ud, vsl + e0, e1 - e0, lane);
+        if (lane == 0) finish(vl, T(dv));
       }
-      if (small && sl == 0) finish(v, T(acc));
-      unsigned long_lists = __ballot_sync(0xffffffffu, valid && !small && sl == 0);
-      while (long_lists) {  // warp-uniform
-        const int sg = (__ffs(long_lists) - 1) / SEG;
-        long_lists &= long_lists - 1;
-        const int vl = vb + sg;
+    }
+    // the queued lists, four per warp: eight lanes and eight registers per list (up to 64
+    // entries, one bitonic network for the four); longer ones warp-wide
+    __syncthreads();
+    const int nq = min(s_nlong, kLongQueue);
+    constexpr int SEG = 8, RQ = 8;
+    const int seg = lane / SEG, sl = lane % SEG;
+    for (;;) {
+      int gi = 0;
+      if (lane == 0) gi = atomicAdd(&s_lnext, 1);
+      const int q0 = 4 * __shfl_sync(0xffffffffu, gi, 0);
+      if (q0 >= nq) break;
+      const bool valid = q0 + seg < nq;
+      const int vq = valid ? s_long[q0 + seg] : 0;
+      int s0 = 0, d = 0;
+      if (valid) {
+        const int s1 = __ldg(vend + vq);
+        s0 = vq > 0 ? __ldg(vend + vq - 1) : 0;
+        d = s1 - s0;
+      }
+      const bool mid = valid && d <= SEG * RQ;
+      double a[RQ];
+#pragma unroll
+      for (int r = 0; r < RQ; r++) {
+        const int e = sl + SEG * r;
+        a[r] = (mid && e < d) ? (P.upos ? ud[s0 + e] : ud[__ldg(vsl + s0 + e)]) : pinf;
+      }
+      const double acc = seg_sort_sum<SEG, RQ>(a, mid ? d : 0, lane);
+      if (mid && sl == 0) finish(vq, T(acc));
+      unsigned big = __ballot_sync(0xffffffffu, valid && !mid && sl == 0);
+      while (big) {  // warp-uniform
+        const int vl = s_long[q0 + (__ffs(big) - 1) / SEG];
+        big &= big - 1;
         const int e1 = __ldg(vend + vl), e0 = vl > 0 ? __ldg(vend + vl - 1) : 0;
         const double dv = P.upos ? sorted_sum<true, int32_t>(ud + e0, nullptr, e1 - e0, lane)
                                  : sorted_sum<false>(ud, vsl + e0, e1 - e0, lane);

@@ -222,6 +222,7 @@ constexpr int kStagedThreads = 1024;  // block size of the staged form
 static int persist_threads(dmm_precision prec) {
   return prec == DMM_FP64 ? kPersistThreads64 : kPersistThreads;
 }
+constexpr int kSlotPad = 8;             // entries past the last slot of vslot and u
 constexpr int kXpSmemMax = 220 * 1024;  // dynamic shared memory of the staged form, at most
 constexpr int kXpMaxTiles = 1 << 14;    // clause or variable tiles of the staged form, at most
 constexpr int kMiscInts = 48;            // misc_d_: 192 bytes
@@ -295,9 +296,10 @@ dmm_status Pack::init(const PackCaps& caps_in, bool with_alpha_cm, bool fixed_gr
   if (with_alpha_cm) DMM_CUDA(dev_alloc(&alpha_cm_, C * tsize_));
   DMM_CUDA(dev_alloc(&coff_, C * 4));
   DMM_CUDA(dev_alloc(&lit_, S * 4));
-  DMM_CUDA(dev_alloc(&vslot_, S * 4));
+  // the per-variable lists are read in aligned 16-byte words: padding past the last slot
+  DMM_CUDA(dev_alloc(&vslot_, (S + kSlotPad) * 4));
   DMM_CUDA(dev_alloc(&upos_, S * 4));
-  DMM_CUDA(dev_alloc(&u_, S * tsize_));
+  DMM_CUDA(dev_alloc(&u_, (S + kSlotPad) * tsize_));
   DMM_CUDA(dev_alloc(&cand_, 2 * kTrials * V * tsize_));
   DMM_CUDA(dev_alloc(&vend_, V * 4));
   DMM_CUDA(dev_alloc(&fill_, V * 4));

@@ -300,3 +300,54 @@ def test_fp64_many_variable_tiles_per_block():
         for r in range(1, 4):
             inst.step(10)
             assert np.array_equal(inst.get_state()[0], ref["dump"][r])
+
+
+def skewed_formula(n, m, a, seed):
+    """3-SAT with variable i drawn with weight (i+1)^-a: occurrence lists from a few entries
+    to hundreds, so one step takes every path of the FP64 sorted sum."""
+    rng = np.random.default_rng(seed)
+    w = 1.0 / np.arange(1, n + 1) ** a
+    w /= w.sum()
+    rows = np.empty((m, 3), np.int64)
+    for c in range(m):
+        rows[c] = rng.choice(np.arange(1, n + 1), size=3, replace=False, p=w)
+    lits = (rows * rng.choice([-1, 1], size=(m, 3))).astype(np.int32).reshape(-1)
+    return lits, np.arange(0, 3 * m + 1, 3, dtype=np.int64)
+
+
+@pytest.mark.parametrize("tuning", [{}, {"var_tile": 64, "clause_tile": 512}])
+def test_fp64_sorted_sum_every_list_length(tuning):
+    """FP64 sums by list length: at most 32 entries (one thread), 33-64 (queued, an 8-lane
+    segment), 65-256 (warp-wide network) and longer (warp-wide selection), on one formula
+    whose lists span all four; per-step states equal the oracle's bit for bit."""
+    n, m = 400, 8000
+    lits, off = skewed_formula(n, m, 0.9, 5)
+    form = dmm.from_arrays(lits, off, n)
+    occ = np.bincount(np.abs(lits), minlength=n + 1)[1:]
+    assert occ.max() > 256 and ((occ > 64) & (occ <= 256)).any()
+    assert ((occ > 32) & (occ <= 64)).any() and (occ <= 32).any()
+    o = Oracle(n, m, lits, off)
+    x0 = uniform_init(n, m, 6)
+    ref = o.run(x0, 25, dump_every=1)
+    with dmm.Instance(form, precision="fp64") as inst:
+        if tuning:
+            inst.set_tuning(**tuning)
+        got, _ = run_steps(inst, x0, 25)
+    assert np.array_equal(got, ref["dump"][: ref["steps"] + 1])
+
+
+def test_fp64_long_list_queue_overflow():
+    """A variable tile with more lists longer than 32 than the block's queue holds (512):
+    the ones past its end are summed in the first pass.  Bit-exact against the oracle."""
+    form, _ = dmm.generate_planted(6_000, 84_000, 0.08, 0.46, seed=21)  # mean list 42
+    occ = np.bincount(np.abs(form.lits), minlength=form.n + 1)[1:]
+    assert (occ[:4096] > 32).sum() > 600
+    o = Oracle(form.n, form.m, form.lits, form.clause_off)
+    x0 = uniform_init(form.n, form.m, 8)
+    ref = o.run(x0, 12, dump_every=4)
+    with dmm.Instance(form, precision="fp64") as inst:
+        inst.set_tuning(var_tile=4096)
+        inst.set_state(x0)
+        for r in range(1, 4):
+            inst.step(4)
+            assert np.array_equal(inst.get_state()[0], ref["dump"][r])
