@@ -128,7 +128,8 @@ __device__ __forceinline__ void add_clause_counts(const PackView<T>& P, TileSmem
   if (sm.acc) {
     if (tu) atomicAdd(&sm.acc->loc, tu);
     if (tv) atomicAdd(&sm.acc->vfail, tv);
-    atomicAdd(&sm.acc->energy, (unsigned long long)et);  // FP32: exact integer units
+    if (sizeof(T) == 4) atomicAdd(&sm.acc->energy, (unsigned long long)et);  // exact units
+    else P.epart[ti] = et;  // FP64: summed in a fixed order (energy_sum)
   } else {
     InstCtrl* S = P.ctrl + sm.tile.inst;
     if (tu) atomicAdd(&S->acc_loc, tu);
@@ -519,11 +520,22 @@ __device__ void commit_step(const PackView<T>& P, const InstDesc& I, int ii, int
 
 // Finalizes one instance's step (block-wide).  Reads the accumulators of the step, writes
 // the new control state, zeroes the accumulators.
+// A formula's energy from its clause tiles' partials, by one warp in a fixed order (lane-
+// strided sums, then a butterfly), so that every launch form reports the same value; valid
+// in every lane.  The partials were written by other blocks before a grid barrier: read
+// past L1.
+template <class T>
+__device__ __forceinline__ double energy_sum(const PackView<T>& P, int ctile0, int nctile) {
+  double e = 0.0;
+  for (int i = threadIdx.x & 31; i < nctile; i += 32) e = __dadd_rn(e, __ldcg(P.epart + ctile0 + i));
+  return warp_sum_d(e);
+}
+
 template <class T, int NT>
 __device__ void finalize_step(const PackView<T>& P, const InstDesc& I, int ii, double* red) {
+  (void)red;
   double e = 0.0;
-  for (int i = threadIdx.x; i < I.nctile; i += NT) e = __dadd_rn(e, P.epart[I.ctile0 + i]);
-  e = block_sum<NT>(e, red);
+  if (threadIdx.x < 32) e = energy_sum(P, I.ctile0, I.nctile);
   if (threadIdx.x == 0) {
     if (sizeof(T) == 4) e = e * (1.0 / kEnergyUnitF32);
     InstCtrl* S = P.ctrl + ii;
@@ -689,7 +701,7 @@ __device__ __forceinline__ void leave_launch(unsigned int* bar) {
 
 // nsteps integration steps in one cooperative launch.  Blocks own tiles statically
 // (tile ti -> block ti % gridDim.x); phases A | B | F are separated by grid barriers.
-// ONE (a single FP32 formula): two grid barriers per step.  The step's counts go to the
+// ONE (a single formula): two grid barriers per step.  The step's counts go to the
 // accumulators acc2[s & 1] (zeroed before the launch; slot (s+1) & 1 is zeroed by block 0
 // once barrier 1 of step s has passed, after every block has read it in step s-1); after
 // barrier 2 every block reads them and applies the step decision to its own copy of the
@@ -769,11 +781,14 @@ __global__ void __launch_bounds__(NT, 1)
     }
     stamp(s, 8);
     if constexpr (ONE) {
+      double e64 = 0.0;  // FP64: the clause tiles' energy partials, summed by warp 0 of block 0
+      if (sizeof(T) == 8 && blockIdx.x == 0 && threadIdx.x < 32)
+        e64 = energy_sum(P, sm.inst.ctile0, sm.inst.nctile);
       if (threadIdx.x == 0) {
         const volatile StepAcc* A = P.acc2 + (s & 1);
         const int loc = A->loc, vfail = A->vfail, kmax = A->kmax;
         if (blockIdx.x == 0) {
-          const double e = (double)A->energy * (1.0 / kEnergyUnitF32);
+          const double e = sizeof(T) == 4 ? (double)A->energy * (1.0 / kEnergyUnitF32) : e64;
           commit_step(P, sm.inst, P.live[0], loc, vfail, kmax, e);
           __threadfence();
         }

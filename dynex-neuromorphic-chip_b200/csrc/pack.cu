@@ -1020,10 +1020,11 @@ static int occupancy_blocks(const void* fn, int threads, size_t smem = 0) {
   return std::max(1, b);
 }
 
-// ONE: single-formula form (FP32 only)
+// ONE: single-formula form
 template <bool ONE>
 static const void* persist_fn_x(dmm_precision prec, int G) {
-  if (prec == DMM_FP64) return (const void*)k_persist<double, 32, true, false, kPersistThreads64>;
+  if (prec == DMM_FP64)
+    return (const void*)k_persist<double, 32, true, false, kPersistThreads64, ONE>;
   switch (G) {
     case 1: return (const void*)k_persist<float, 1, false, true, kPersistThreads, ONE>;
     case 2: return (const void*)k_persist<float, 2, false, true, kPersistThreads, ONE>;
@@ -1314,10 +1315,11 @@ dmm_status Pack::commit_tiles() {
     set_error("tile tables overflow");
     return DMM_ERR_BUDGET;
   }
-  // one FP32 formula on the cooperative path: two grid barriers per step; with the
-  // default layout and tiles, the staged form when it fits
-  one_active_ = coop && prec_ == DMM_FP32 && live_list.size() == 1 && small_list.empty();
-  if (one_active_ && tun_.u_layout == 0 && tun_.clause_tile == 0 && tun_.var_tile == 0) {
+  // one formula on the cooperative path: two grid barriers per step; FP32 with the
+  // default layout and tiles: the staged form when it fits
+  one_active_ = coop && live_list.size() == 1 && small_list.empty();
+  if (one_active_ && prec_ == DMM_FP32 && tun_.u_layout == 0 && tun_.clause_tile == 0 &&
+      tun_.var_tile == 0) {
     DMM_TRY(prepare_xpose(live_list[0], TC, TV, false, &xp_active_));
     // too large for one tile per block: several tiles per block, else the tiles above
     if (!xp_active_) {
@@ -1528,6 +1530,7 @@ dmm_status Pack::preload_kernels() {
     fns.push_back((const void*)k_set_state<double>);
     fns.push_back((const void*)k_get_state<double>);
     fns.push_back((const void*)k_signs<double>);
+    fns.push_back(persist_fn_x<true>(prec_, G));
   } else {
     fns.push_back((const void*)k_set_state<float>);
     fns.push_back((const void*)k_get_state<float>);

@@ -160,7 +160,7 @@ def test_full_size_fp64_bitexact_vs_oracle_first_steps(big):
     o = Oracle(form.n, form.m, form.lits, form.clause_off, precision="fp64")
     ref = o.run(x0, 6, dump_every=3)
     with dmm.Instance(form, precision="fp64") as inst:
-        assert inst.launch_form == "cooperative"
+        assert inst.launch_form == "cooperative-single"
         inst.set_state(x0)
         for r in range(1, 3):
             inst.step(3)

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("prec,layout,form_want", [("fp32", 0, "staged"),
                                                     ("fp32", 1, "cooperative-single"),
-                                                    ("fp64", 0, "cooperative")])
+                                                    ("fp64", 0, "cooperative-single")])
 def test_barrier_wait_gives_up_and_instance_recovers(prec, layout, form_want):
     form, _ = dmm.generate_planted(3_000, 12_600, 0.08, 0.46, seed=31)
     x0 = dmm.initial_state_uniform(form, 32)

@@ -177,8 +177,7 @@ def test_contribution_layout_does_not_change_results(fixtures, prec):
         with dmm.Instance(formula(f), precision=prec) as inst:
             inst.set_tuning(u_layout=lay, launch_mode=mode)
             if mode == 0:  # the staged kernel is the FP32 default layout's
-                want = "staged" if prec == "fp32" and lay == 0 else (
-                    "cooperative-single" if prec == "fp32" else "cooperative")
+                want = "staged" if prec == "fp32" and lay == 0 else "cooperative-single"
                 assert inst.launch_form == want
             inst.set_state(x0)
             inst.step(120)
