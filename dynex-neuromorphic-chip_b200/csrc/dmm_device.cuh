@@ -96,6 +96,7 @@ struct PackView {
   int32_t* ring_tail;
   int32_t ring_cap;
   const int32_t* live;      // indices of the instances with tiles
+  int32_t live0;            // live[0] when the host knows it (single-formula forms), else -1
   const int32_t* nlive;
   const int32_t* upos;      // variable-major position of each slot (null: u is slot-major)
   StepAcc* acc2;            // [2] step accumulators of the single-formula cooperative form

@@ -259,6 +259,7 @@ class Pack {
   int64_t xbuf_cap_[kXpBufs] = {};
   int32_t xsv_cap_ = 0, xbk_cap_ = 0, xtv_cap_ = 0, xst_cap_ = 0, xsmem_ = 0;
   bool xp_mt_ = false;  // the staged form runs several tiles per block
+  int32_t live0_ = -1;  // the live formula when exactly one has tiles
   long long* trace_ = nullptr;
   int64_t trace_cap_ = 0;
   bool trace_on_ = false;

@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(NT, 1)
   const int b = blockIdx.x, tid = threadIdx.x;
   const int nct = P.ntiles[0], nvt = P.ntiles[1];
   const bool has_c = b < nct, has_v = b < nvt;
-  const int ii = P.live[0];
+  const int ii = P.live0 >= 0 ? P.live0 : P.live[0];
   L2Pol pol{0, 0};
   if constexpr (MT) pol = make_l2pol(P.xl2_plain != 0);
 
@@ -285,14 +285,28 @@ __global__ void __launch_bounds__(NT, 1)
   }
   __syncthreads();
   if (!MT && has_v) {
+    // phase B's tables arrive by asynchronous copies that the first wait of phase A
+    // completes, so they load alongside phase A's first reads: the raw CSR ends (s_vend[0]
+    // = the end before the tile, subtracted where they are read) and the unit pins as
+    // 4-byte words (the tile starts at a multiple of 4 variables of a 32-aligned range,
+    // and the pin array has slack past its last variable)
     const int32_t* vend = P.vend + I.var0;
-    const int jb = vtile.begin > 0 ? __ldg(vend + vtile.begin - 1) : 0;
-    for (int g = tid; g < blen / 8; g += NT) s_src8[g] = __ldg(P.xsrc8 + bbeg / 8 + g);
-    for (int i = tid; i <= vtile.count; i += NT)
-      s_vend[i] = i == 0 ? 0 : __ldg(vend + vtile.begin + i - 1) - jb;
-    for (int i = tid; i < vtile.count; i += NT) s_unit[i] = P.unit[I.var0 + vtile.begin + i];
+    for (int g = tid; g < blen / 8; g += NT) cp_async4(s_src8 + g, P.xsrc8 + bbeg / 8 + g);
+    for (int i = tid; i <= vtile.count; i += NT) {
+      if (i > 0 || vtile.begin > 0) cp_async4(s_vend + i, vend + vtile.begin + i - 1);
+      else s_vend[0] = 0;
+    }
+    for (int w = tid; 4 * w < vtile.count; w += NT)
+      cp_async4(s_unit + 4 * w, P.unit + I.var0 + vtile.begin + 4 * w);
   }
-  cp_async_wait_all();
+  if (!MT && tid == 32 && lc.done == 0) {
+    // the voltages of the first step: this block's share of them toward L2 (later steps
+    // read the candidates the previous step wrote, still in L2)
+    const T* V0 = P.cand + (int64_t)(lc.set * kTrials + lc.kcur) * P.var_cap + I.var0;
+    const int64_t per = ((int64_t)I.n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = min((int64_t)I.n, per * b), hi = min((int64_t)I.n, lo + per);
+    if (hi > lo) prefetch_l2(V0, 4 * lo, 4 * hi, 0);
+  }
   __syncthreads();
 
   unsigned int target = 0;
@@ -613,8 +627,8 @@ __global__ void __launch_bounds__(NT, 1)
         const bool valid = i < nv;
         int s0 = 0, s1 = 0;
         if (valid) {
-          s0 = s_vend[i];
-          s1 = s_vend[i + 1];
+          s0 = s_vend[i] - s_vend[0];
+          s1 = s_vend[i + 1] - s_vend[0];
         }
         const T dv = tree_sum<T, G, true, int32_t>(bucket + s0, nullptr, s1 - s0, lane);
         if constexpr (G >= kTrials) {

@@ -928,6 +928,7 @@ void Pack::fill_view(void* vv) const {
   v.ring_tail = ring_tail_d_;
   v.ring_cap = caps_.insts;
   v.live = live_d_;
+  v.live0 = live0_;
   v.nlive = misc_d_;
   v.acc2 = reinterpret_cast<StepAcc*>(misc_d_ + kMiscAcc2);
   // tile paths: slot-major unless asked (measured faster there); the one-block-per-formula
@@ -1333,6 +1334,7 @@ dmm_status Pack::commit_tiles() {
   if (!vtiles_h_.empty())
     DMM_CUDA(cudaMemcpyAsync(vtiles_d_, vtiles_h_.data(), vtiles_h_.size() * sizeof(Tile),
                              cudaMemcpyHostToDevice, stream_));
+  live0_ = live_list.size() == 1 ? live_list[0] : -1;
   if (!live_list.empty())
     DMM_CUDA(cudaMemcpyAsync(live_d_, live_list.data(), live_list.size() * sizeof(int32_t),
                              cudaMemcpyHostToDevice, stream_));
