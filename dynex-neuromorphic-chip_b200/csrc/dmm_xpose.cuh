@@ -369,6 +369,19 @@ __global__ void __launch_bounds__(NT, 1)
       for (int i = tid; i < dcnt; i += NT) cp_async4(sV + i, V + sVi[i]);
       const int c_begin = ctile.begin, c_end = ctile.begin + ctile.count;
       const int g0 = c_begin + 4 * tid;
+      if (!MT && s == 0 && (tid >> 5) == 1) {
+        // first step of a launch, when the tables may be cold: while the voltages gather,
+        // one warp asks L2 for the tile's local literals, staging positions and clause
+        // memories (read next) and for phase B's bucket destinations
+        const int64_t c0 = c_begin, c1 = c_end;
+        prefetch_l2(P.xllit, 6 * c0, 6 * c1, tid & 31);
+        prefetch_l2(P.xspos, 6 * c0, 6 * c1, tid & 31);
+        prefetch_l2(P.Xs + I.cls0, 4 * c0, 4 * c1, tid & 31);
+        prefetch_l2(P.Xl + I.cls0, 4 * c0, 4 * c1, tid & 31);
+        if (pending) prefetch_l2(P.Cp + I.cls0, 4 * c0, 4 * c1, tid & 31);
+        if (I.has_alpha_cm) prefetch_l2(P.alpha_cm + I.cls0, 4 * c0, 4 * c1, tid & 31);
+        if (has_v) prefetch_l2(P.xdst, 2 * (int64_t)bbeg, 2 * ((int64_t)bbeg + blen), tid & 31);
+      }
       cp_async_wait_all();
       __syncthreads();
       trace_stamp(P, s, 2);
