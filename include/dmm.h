@@ -244,7 +244,8 @@ dmm_status dmm_instance_assignment(dmm_instance* inst, int8_t* pre, int8_t* post
  * this instance with its current tuning:
  *   1  two kernels per step (clause tiles, then variable tiles), CUDA graphs
  *   2  one cooperative kernel for several steps, three grid barriers per step
- *   3  the same for a single FP32 formula: two grid barriers per step
+ *   3  the same for a single formula (FP64, or FP32 without the staged tables): two grid
+ *      barriers per step
  *   4  the staged single-formula kernel (FP32, 3-literal clauses, tables fit)
  *   6  the staged kernel with several clause and variable tiles per block (formulas whose
  *      tiles are too large for one of each per block)
