@@ -28,7 +28,7 @@ namespace numeric {
 namespace odeint {
 
 [[noreturn]] inline void odeint_stub_abort(const char* what) {
-  std::fprintf(stderr, "odeint stub: %s is not available in this build\n", what);
+  std::fprintf(stderr, "odeint stub: %s is not provided by this stub\n", what);
   std::abort();
 }
 

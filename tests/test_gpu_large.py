@@ -7,7 +7,7 @@ long per-variable lists, which only appear at the benchmarked sizes:
   (SHA-256, every 25 steps) until it solves, with the same solve step, T and assignments;
 * n = 100,000 with the fixtures' literal split, which does not solve within 1000 steps:
   FP64 equal to the reference for 1000 steps and FP32 equal to the oracle's FP32
-  restatement for 1000 steps (hashes every 50 steps) -- the north-star tolerance is 1e-12
+  restatement for 1000 steps (hashes every 50 steps) -- the required tolerance is 1e-12
   relative over the first 1000 steps, and the states are bit-identical;
 * n = 1,000,000, m = 8,000,000: the first 8 steps of both precisions (a hash per step);
 * the reference's n = 10000 fixture through the `dynex` command line: its known answer.

@@ -1,5 +1,5 @@
 """GPU parity: the CUDA path through the C ABI against the oracle and the reference's
-golden answers.  FP64 mode is compared bit for bit (the north-star tolerance is 1e-12
+golden answers.  FP64 mode is compared bit for bit (the required tolerance is 1e-12
 relative per step; the implementation reproduces the reference's arithmetic exactly).
 FP32 mode is compared bit for bit against the oracle's FP32 restatement, and against FP64
 within stated per-horizon bounds."""
