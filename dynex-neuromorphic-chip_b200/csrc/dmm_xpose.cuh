@@ -771,6 +771,7 @@ __global__ void __launch_bounds__(NT, 1)
     }
     trace_stamp(P, s, 9);
   }
+  cp_async_wait_all();  // a launch on a finished formula left the prologue's copies pending
   leave_launch(bar);
   trace_launch(P, 1);
 }
