@@ -8,7 +8,13 @@
 #include <cstring>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "dmm_pack.h"
 
@@ -68,11 +74,161 @@ static dmm_status alloc_cnf(int32_t n, int32_t m, int64_t nlits, dmm_cnf** out) 
   return DMM_OK;
 }
 
-static void occurrences(dmm_cnf* c) {
+// ---- clause section of a DIMACS file, tokenized in chunks --------------------------------
+//
+// The clause section is cut at line starts into chunks that threads tokenize on their own:
+// each turns its tokens into values (a `c` token skips the rest of its line, which never
+// crosses a chunk) and stops at its first token that is not a literal, recording it.  The
+// tokens of all chunks in order are the tokens the sequential reader sees, so one pass over
+// them afterwards applies the clause rules in file order and stops after the m-th clause;
+// a chunk's recorded error counts only if that pass reaches it.
+
+inline bool is_ws(char c) {
+  return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\f' || c == '\v';
+}
+
+struct CnfChunk {
+  std::vector<int32_t> vals;  // literal values and 0 terminators, in file order
+  int end = 0;                // what follows vals: 0 the chunk's end, 1 a token that is not
+                              // an integer (bad_tok), 2 an integer beyond int32 (big)
+  std::string bad_tok;
+  int64_t big = 0;
+};
+
+// Tokenizes [p, e): integers as strtoll reads them (optional sign, decimal digits, the whole
+// token; values beyond int64 saturate as strtoll's do), `c` tokens skip to the end of the
+// line; a token that is not an integer, or an integer outside int32 (never a literal),
+// ends the chunk.
+static void tokenize_chunk(const char* p, const char* e, CnfChunk* out) {
+  std::vector<int32_t>& v = out->vals;
+  v.reserve((size_t)(e - p) / 6 + 16);
+  while (p < e) {
+    while (p < e && is_ws(*p)) p++;
+    if (p >= e) break;
+    const char* tb = p;
+    while (p < e && !is_ws(*p)) p++;
+    const char* te = p;
+    if (te - tb == 1 && *tb == 'c') {
+      while (p < e && *p != '\n') p++;
+      continue;
+    }
+    const char* q = tb;
+    bool neg = false;
+    if (*q == '+' || *q == '-') neg = *q++ == '-';
+    if (q == te) {
+      out->end = 1;
+      out->bad_tok.assign(tb, te);
+      return;
+    }
+    uint64_t x = 0;
+    bool sat = false;
+    for (; q < te; q++) {
+      const unsigned d = (unsigned)(*q - '0');
+      if (d > 9) {
+        out->end = 1;
+        out->bad_tok.assign(tb, te);
+        return;
+      }
+      if (x > (UINT64_MAX - d) / 10) sat = true;
+      else x = 10 * x + d;
+    }
+    int64_t val;
+    if (neg) val = (sat || x > (uint64_t)INT64_MAX + 1) ? INT64_MIN : (int64_t)(0 - x);
+    else val = (sat || x > (uint64_t)INT64_MAX) ? INT64_MAX : (int64_t)x;
+    if (val > INT32_MAX || val < -(int64_t)INT32_MAX) {
+      out->end = 2;
+      out->big = val;
+      return;
+    }
+    v.push_back((int32_t)val);
+  }
+}
+
+// Runs f(k) for k in [0, count) on up to `count` threads (this one included).
+template <class F>
+static void parallel_for(int count, F f) {
+  std::vector<std::thread> pool;
+  for (int k = 1; k < count; k++) pool.emplace_back(f, k);
+  if (count > 0) f(0);
+  for (auto& t : pool) t.join();
+}
+
+// Literal and clause counts of a chunk's values: zeros, non-zeros, and the non-zeros after
+// its last zero (all of them when it has none).
+struct ChunkCounts {
+  int64_t zeros = 0, lits = 0, trailing = 0;
+};
+static ChunkCounts count_chunk(const std::vector<int32_t>& v) {
+  ChunkCounts c;
+  for (const int32_t x : v) {
+    if (x == 0) {
+      c.zeros++;
+      c.trailing = 0;
+    } else {
+      c.lits++;
+      c.trailing++;
+    }
+  }
+  return c;
+}
+
+// A file's bytes: mapped read-only when possible, else read into memory.
+struct FileBytes {
+  const char* p = nullptr;
+  size_t n = 0;
+  void* map = nullptr;
+  std::vector<char> buf;
+  ~FileBytes() {
+    if (map) munmap(map, n);
+  }
+  bool open(const char* path) {
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat sb;
+    if (fstat(fd, &sb) == 0 && S_ISREG(sb.st_mode) && sb.st_size > 0) {
+      void* m = mmap(nullptr, (size_t)sb.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (m != MAP_FAILED) {
+        map = m;
+        n = (size_t)sb.st_size;
+        p = static_cast<const char*>(m);
+        ::close(fd);
+        return true;
+      }
+    }
+    char tmp[1 << 16];
+    for (;;) {
+      const ssize_t r = ::read(fd, tmp, sizeof tmp);
+      if (r < 0) {
+        ::close(fd);
+        return false;
+      }
+      if (r == 0) break;
+      buf.insert(buf.end(), tmp, tmp + r);
+    }
+    ::close(fd);
+    p = buf.data();
+    n = buf.size();
+    return true;
+  }
+};
+
+// Largest occurrence count of a variable; `threads` > 1 counts slices of the literals in
+// parallel with atomic increments (the counts, and so the result, do not depend on it).
+static void occurrences(dmm_cnf* c, int threads = 1) {
   std::vector<int32_t> occ(c->n + 1, 0);
-  int32_t mx = 0;
-  for (int64_t i = 0; i < c->nlits; i++) mx = std::max(mx, ++occ[std::abs(c->lits[i])]);
-  c->max_occurrence = mx;
+  if (threads <= 1 || c->nlits < (1 << 20)) {
+    int32_t mx = 0;
+    for (int64_t i = 0; i < c->nlits; i++) mx = std::max(mx, ++occ[std::abs(c->lits[i])]);
+    c->max_occurrence = mx;
+    return;
+  }
+  int32_t* o = occ.data();
+  const int64_t per = (c->nlits + threads - 1) / threads;
+  parallel_for(threads, [&](int k) {
+    const int64_t lo = std::min(c->nlits, per * k), hi = std::min(c->nlits, lo + per);
+    for (int64_t i = lo; i < hi; i++) __atomic_fetch_add(o + std::abs(c->lits[i]), 1, __ATOMIC_RELAXED);
+  });
+  c->max_occurrence = *std::max_element(occ.begin(), occ.end());
 }
 
 }  // namespace dmm
@@ -92,41 +248,24 @@ void dmm_cnf_free(dmm_cnf* c) {
 // `p cnf n m`, then m clauses of 0-terminated literals where a `c` token inside the
 // clause section skips the rest of its line.  A clause longer than DMM_MAX_CLAUSE_LITS is
 // an error as in the reference.  A file that ends before m clauses is an error here
-// (the reference would read empty clauses).
+// (the reference would read empty clauses).  Whatever follows the m-th clause is not read.
+// The clause section is tokenized and checked in chunks on several threads; the result,
+// and the error reported (the first in file order), are those of reading it in sequence.
 dmm_status dmm_cnf_read(const char* path, dmm_cnf** out) {
   clear_error();
   if (!path || !out) return DMM_ERR_ARG;
-  FILE* f = std::fopen(path, "rb");
-  if (!f) {
+  FileBytes file;
+  if (!file.open(path)) {
     set_error("cannot open %s", path);
     return DMM_ERR_IO;
   }
-  std::string buf;
-  {
-    std::fseek(f, 0, SEEK_END);
-    long sz = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    if (sz < 0) sz = 0;
-    buf.resize((size_t)sz);
-    if (sz > 0 && std::fread(&buf[0], 1, (size_t)sz, f) != (size_t)sz) {
-      std::fclose(f);
-      set_error("read error on %s", path);
-      return DMM_ERR_IO;
-    }
-    std::fclose(f);
-  }
-  const char* p = buf.data();
-  const char* e = p + buf.size();
-  auto skip_ws = [&]() {
-    while (p < e && (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r' || *p == '\f' || *p == '\v'))
-      p++;
-  };
+  const char* p = file.p;
+  const char* e = p + file.n;
   auto token = [&](const char** b, const char** te) -> bool {
-    skip_ws();
+    while (p < e && is_ws(*p)) p++;
     if (p >= e) return false;
     *b = p;
-    while (p < e && !(*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r' || *p == '\f' || *p == '\v'))
-      p++;
+    while (p < e && !is_ws(*p)) p++;
     *te = p;
     return true;
   };
@@ -157,48 +296,128 @@ dmm_status dmm_cnf_read(const char* path, dmm_cnf** out) {
     set_error("%s: bad header n=%lld m=%lld", path, nn, mm);
     return DMM_ERR_PARSE;
   }
-  std::vector<int32_t> lits;
-  std::vector<int64_t> off;
-  lits.reserve((size_t)mm * 3);
-  off.reserve((size_t)mm + 1);
-  off.push_back(0);
-  for (long long i = 0; i < mm; i++) {
-    int len = 0;
-    for (;;) {
-      if (!token(&tb, &te)) {
-        set_error("%s: file ends after %lld of %lld clauses", path, i, mm);
-        return DMM_ERR_PARSE;
-      }
-      if (te - tb == 1 && *tb == 'c') {
-        while (p < e && *p != '\n') p++;
+  // the clause section in chunks cut at line starts (one per MB at least, at most 32),
+  // tokenized by one thread each
+  const size_t rest = (size_t)(e - p);
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nchunk =
+      (int)std::min<size_t>({(size_t)std::min(hw, 32u), rest / (1u << 20) + 1});
+  std::vector<const char*> cut(nchunk + 1);
+  cut[0] = p;
+  cut[nchunk] = e;
+  for (int k = 1; k < nchunk; k++) {
+    const char* q = std::max(cut[k - 1], p + rest / nchunk * k);
+    while (q < e && *q != '\n') q++;
+    cut[k] = q < e ? q + 1 : e;
+  }
+  std::vector<CnfChunk> chunks(nchunk);
+  std::vector<ChunkCounts> cnt(nchunk);
+  parallel_for(nchunk, [&](int k) {
+    tokenize_chunk(cut[k], cut[k + 1], &chunks[k]);
+    cnt[k] = count_chunk(chunks[k].vals);
+  });
+  // where each chunk starts: its first clause, its first literal, and the literals of the
+  // clause open at its start (for the length rule); the chunk that holds the m-th clause end
+  // and the values of it up to there
+  std::vector<int64_t> c0(nchunk + 1, 0), l0(nchunk + 1, 0), open(nchunk + 1, 0);
+  for (int k = 0; k < nchunk; k++) {
+    c0[k + 1] = c0[k] + cnt[k].zeros;
+    l0[k + 1] = l0[k] + cnt[k].lits;
+    open[k + 1] = cnt[k].zeros > 0 ? cnt[k].trailing : open[k] + cnt[k].lits;
+  }
+  int last = nchunk - 1;  // the last chunk read
+  size_t used_last = chunks[last].vals.size();
+  for (int k = 0; k < nchunk; k++) {
+    if (c0[k + 1] >= mm) {
+      last = k;
+      int64_t z = c0[k];
+      size_t j = 0;
+      const std::vector<int32_t>& v = chunks[k].vals;
+      while (z < mm) z += v[j++] == 0;  // past the m-th clause's terminator
+      used_last = j;
+      break;
+    }
+  }
+  // every chunk up to `last` checks the clause rules on its values and writes its literals
+  // and clause ends in place; the first violation in file order is the one reported
+  struct Fault {
+    size_t at = SIZE_MAX;  // value index of the chunk
+    int kind = 0;          // 1 literal out of range, 2 clause too long
+    int64_t clause = 0;
+    long long value = 0;
+  };
+  std::vector<Fault> fault(nchunk);
+  const bool complete = c0[nchunk] >= mm;
+  const int64_t nlits = complete ? l0[last] + [&] {
+    int64_t c = 0;
+    for (size_t j = 0; j < used_last; j++) c += chunks[last].vals[j] != 0;
+    return c;
+  }() : 0;
+  // (a file that ends early is still checked: a violation before its end is reported as
+  // such, as the sequential reading would)
+  dmm_cnf* c = nullptr;
+  if (complete) {
+    dmm_status st = alloc_cnf((int32_t)nn, (int32_t)mm, nlits, &c);
+    if (st != DMM_OK) return st;
+    c->clause_off[0] = 0;
+  }
+  parallel_for(last + 1, [&](int k) {
+    const std::vector<int32_t>& v = chunks[k].vals;
+    const size_t nv = k == last ? used_last : v.size();
+    int64_t cl = c0[k], li = l0[k], len = open[k];
+    for (size_t j = 0; j < nv; j++) {
+      const int32_t x = v[j];
+      if (x == 0) {
+        cl++;
+        if (c) c->clause_off[cl] = li;
+        len = 0;
         continue;
       }
-      char* endp = nullptr;
-      std::string tok(tb, te);
-      const long long v = std::strtoll(tok.c_str(), &endp, 10);
-      if (endp == tok.c_str() || *endp != '\0') {
-        set_error("%s: bad literal `%s` in clause %lld", path, tok.c_str(), i);
-        return DMM_ERR_PARSE;
-      }
-      if (v == 0) break;
-      if (v > nn || v < -nn) {
-        set_error("%s: literal %lld out of range in clause %lld", path, v, i);
-        return DMM_ERR_LITERAL;
+      if (x > nn || x < -nn) {
+        fault[k] = {j, 1, cl, (long long)x};
+        return;
       }
       if (++len > DMM_MAX_CLAUSE_LITS) {
-        set_error("CLAUSE %lld HAS MORE THAN %d LITERALS.", i, DMM_MAX_CLAUSE_LITS);
-        return DMM_ERR_CLAUSE_LEN;
+        fault[k] = {j, 2, cl, 0};
+        return;
       }
-      lits.push_back((int32_t)v);
+      if (c) c->lits[li] = x;
+      li++;
     }
-    off.push_back((int64_t)lits.size());
+  });
+  // the first violation in file order: a clause rule, or the token that ended a chunk
+  for (int k = 0; k <= last; k++) {
+    const Fault& f = fault[k];
+    if (f.kind == 1 || f.kind == 2) {
+      dmm_cnf_free(c);
+      if (f.kind == 1) {
+        set_error("%s: literal %lld out of range in clause %lld", path, f.value,
+                  (long long)f.clause);
+        return DMM_ERR_LITERAL;
+      }
+      set_error("CLAUSE %lld HAS MORE THAN %d LITERALS.", (long long)f.clause,
+                DMM_MAX_CLAUSE_LITS);
+      return DMM_ERR_CLAUSE_LEN;
+    }
+    const bool ends_here = !(complete && k == last);  // the m-th clause ended before it
+    if (ends_here && chunks[k].end == 1) {
+      dmm_cnf_free(c);
+      set_error("%s: bad literal `%s` in clause %lld", path, chunks[k].bad_tok.c_str(),
+                (long long)c0[k + 1]);
+      return DMM_ERR_PARSE;
+    }
+    if (ends_here && chunks[k].end == 2) {
+      dmm_cnf_free(c);
+      set_error("%s: literal %lld out of range in clause %lld", path, (long long)chunks[k].big,
+                (long long)c0[k + 1]);
+      return DMM_ERR_LITERAL;
+    }
   }
-  dmm_cnf* c = nullptr;
-  dmm_status st = alloc_cnf((int32_t)nn, (int32_t)mm, (int64_t)lits.size(), &c);
-  if (st != DMM_OK) return st;
-  std::memcpy(c->lits, lits.data(), lits.size() * sizeof(int32_t));
-  std::memcpy(c->clause_off, off.data(), off.size() * sizeof(int64_t));
-  occurrences(c);
+  if (!complete) {
+    set_error("%s: file ends after %lld of %lld clauses", path, (long long)c0[nchunk], mm);
+    return DMM_ERR_PARSE;
+  }
+  occurrences(c, nchunk);
   *out = c;
   return DMM_OK;
 }
