@@ -144,11 +144,17 @@ static void tokenize_chunk(const char* p, const char* e, CnfChunk* out) {
   }
 }
 
-// Runs f(k) for k in [0, count) on up to `count` threads (this one included).
+// Runs f(k) for k in [0, count) on up to `count` threads (this one included); the tasks
+// whose thread cannot be started run on this thread.
 template <class F>
 static void parallel_for(int count, F f) {
   std::vector<std::thread> pool;
-  for (int k = 1; k < count; k++) pool.emplace_back(f, k);
+  int started = 1;
+  try {
+    for (; started < count; started++) pool.emplace_back(f, started);
+  } catch (...) {
+  }
+  for (int k = started; k < count; k++) f(k);
   if (count > 0) f(0);
   for (auto& t : pool) t.join();
 }
