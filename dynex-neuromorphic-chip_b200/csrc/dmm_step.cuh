@@ -518,12 +518,11 @@ __device__ void commit_step(const PackView<T>& P, const InstDesc& I, int ii, int
   }
 }
 
-// Finalizes one instance's step (block-wide).  Reads the accumulators of the step, writes
-// the new control state, zeroes the accumulators.
 // A formula's energy from its clause tiles' partials, by one warp in a fixed order (lane-
-// strided sums, then a butterfly), so that every launch form reports the same value; valid
-// in every lane.  The partials were written by other blocks before a grid barrier: read
-// past L1.
+// strided sums, then a butterfly), the same in the single-formula and the multi-formula
+// cooperative forms: for a given tiling the value does not depend on the form (FP32
+// partials are exact integers, so there it does not depend on the tiling either); valid in
+// every lane.  The partials were written by other blocks before a grid barrier: read past L1.
 template <class T>
 __device__ __forceinline__ double energy_sum(const PackView<T>& P, int ctile0, int nctile) {
   double e = 0.0;
@@ -531,6 +530,8 @@ __device__ __forceinline__ double energy_sum(const PackView<T>& P, int ctile0, i
   return warp_sum_d(e);
 }
 
+// Finalizes one instance's step (block-wide).  Reads the accumulators of the step, writes
+// the new control state, zeroes the accumulators.
 template <class T, int NT>
 __device__ void finalize_step(const PackView<T>& P, const InstDesc& I, int ii, double* red) {
   (void)red;
