@@ -314,3 +314,31 @@ def test_cooperative_batch_with_formulas_finishing_at_different_steps():
         assert len(steps) > 10  # the formulas finish at many different steps
     finally:
         b.close()
+
+
+def test_fp64_energy_same_alone_and_in_a_batch_with_the_same_tiles(fixtures):
+    """FP64 energies are sums of per-tile partials: with the same clause and variable tiles,
+    a formula alone (single-formula cooperative form) and in a batch of two (multi-formula
+    form) report the same energy, bit for bit, and the same state."""
+    f, g = fixtures["n500"], fixtures["n1000"]
+    form, other = formula(f), formula(g)
+    x0, x1 = uniform_init(f["n"], f["m"], 41), uniform_init(g["n"], g["m"], 42)
+    tiles = dict(clause_tile=512, var_tile=64)
+    with dmm.Instance(form, precision="fp64") as inst:
+        inst.set_tuning(**tiles)
+        assert inst.launch_form == "cooperative-single"
+        inst.set_state(x0)
+        r_a = inst.step(30)
+        x_a = inst.get_state()[0]
+    b = dmm.Batch.for_formulas([form, other], precision="fp64")
+    try:
+        b.set_tuning(**tiles)
+        b.add(form, x0, max_steps=30)
+        b.add(other, x1, max_steps=30)
+        b.run()
+        r_b, _ = b.result(0)
+        assert (r_b.steps, r_b.t, r_b.loc) == (r_a.steps, r_a.t, r_a.loc)
+        assert r_b.energy == r_a.energy
+        assert np.array_equal(b.state(0)[0], x_a)
+    finally:
+        b.close()
