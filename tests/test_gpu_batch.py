@@ -342,3 +342,28 @@ def test_fp64_energy_same_alone_and_in_a_batch_with_the_same_tiles(fixtures):
         assert np.array_equal(b.state(0)[0], x_a)
     finally:
         b.close()
+
+
+def test_one_block_per_formula_with_contributions_in_global_memory():
+    """One block per formula (launch mode 3) for formulas whose contributions do not fit in
+    the block's shared memory (more than 36,864 literal slots: slot-major in global memory)
+    and for ones that do (variable-major in shared memory), mixed in one batch: every
+    formula's state and report equal its run alone."""
+    sizes = [(5000, 40000), (8000, 20000), (1000, 8000), (4000, 12300), (4096, 12288)]
+    forms = [dmm.generate_planted(n, m, 0.08, 0.46, seed=60 + k)[0] for k, (n, m) in enumerate(sizes)]
+    x0s = [dmm.initial_state_uniform(f, 70 + k) for k, f in enumerate(forms)]
+    b = dmm.Batch.for_formulas(forms, precision="fp32")
+    try:
+        b.set_tuning(launch_mode=3)
+        for f, x0 in zip(forms, x0s):
+            b.add(f, x0, max_steps=150)
+        b.run()
+        for k, (f, x0) in enumerate(zip(forms, x0s)):
+            r_b, post_b = b.result(k)
+            r_a, post_a, x_a = alone(f, x0, "fp32", 150)
+            assert (r_b.status, r_b.steps, r_b.solved_step, r_b.t, r_b.loc) == (
+                r_a.status, r_a.steps, r_a.solved_step, r_a.t, r_a.loc)
+            assert np.array_equal(b.state(k)[0], x_a)
+            assert np.array_equal(post_b, post_a)
+    finally:
+        b.close()
