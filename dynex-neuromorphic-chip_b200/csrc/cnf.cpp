@@ -1,6 +1,7 @@
 // Host-side formula handling: DIMACS reader/writer, planted generator, strict-sign
 // checker and initial states.
 #include <algorithm>
+#include <charconv>
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -453,17 +454,42 @@ dmm_status dmm_cnf_write(const dmm_cnf* c, const char* path, const int8_t* plant
     set_error("cannot write %s", path);
     return DMM_ERR_IO;
   }
+  // the text in blocks of about 1 MB: integers formatted with to_chars, one fwrite per block
+  std::vector<char> buf(1 << 20);
+  size_t used = 0;
+  bool ok = true;
+  auto flush = [&]() {
+    if (used && std::fwrite(buf.data(), 1, used, f) != used) ok = false;
+    used = 0;
+  };
+  auto put = [&](const char* s, size_t len) {
+    if (used + len > buf.size()) flush();
+    std::memcpy(buf.data() + used, s, len);
+    used += len;
+  };
+  auto put_int = [&](long long v, char sep_before, char sep_after) {
+    if (used + 24 > buf.size()) flush();
+    char* q = buf.data() + used;
+    if (sep_before) *q++ = sep_before;
+    q = std::to_chars(q, q + 21, v).ptr;
+    if (sep_after) *q++ = sep_after;
+    used = (size_t)(q - buf.data());
+  };
   if (planted) {
-    std::fprintf(f, "c [");
-    for (int32_t i = 0; i < c->n; i++) std::fprintf(f, " %d", planted[i] > 0 ? i + 1 : -(i + 1));
-    std::fprintf(f, " ]\n");
+    put("c [", 3);
+    for (int32_t i = 0; i < c->n; i++) put_int(planted[i] > 0 ? i + 1 : -(i + 1), ' ', 0);
+    put(" ]\n", 3);
   }
-  std::fprintf(f, "p cnf %d %d\n", c->n, c->m);
+  char head[64];
+  const int hl = std::snprintf(head, sizeof head, "p cnf %d %d\n", c->n, c->m);
+  put(head, (size_t)hl);
   for (int32_t i = 0; i < c->m; i++) {
-    for (int64_t j = c->clause_off[i]; j < c->clause_off[i + 1]; j++) std::fprintf(f, "%d ", c->lits[j]);
-    std::fprintf(f, "0\n");
+    for (int64_t j = c->clause_off[i]; j < c->clause_off[i + 1]; j++) put_int(c->lits[j], 0, ' ');
+    put("0\n", 2);
   }
-  const bool ok = std::fclose(f) == 0;
+  flush();
+  ok = std::fclose(f) == 0 && ok;
+  if (!ok) set_error("write error on %s", path);
   return ok ? DMM_OK : DMM_ERR_IO;
 }
 

@@ -158,3 +158,21 @@ def test_reader_small_and_empty_cases(tmp_path):
                  b"p cnf 3 2\n1 -2\n 3 0 -1 c x\n 0\n", b"p cnf 3 1\n-0\n", b"p cnf 3 1\n",
                  b"c only\n", b"p dnf 3 1\n1 0\n", b"p cnf 3 1\n1 2 3"]:
         check(tmp_path, text)
+
+
+def test_writer_text_layout(tmp_path):
+    """dmm_cnf_write: the planted comment line, the header, then one clause per line as
+    `l1 l2 l3 0`, exactly; a large file reads back to the same formula."""
+    f, planted = dmm.generate_planted(300, 1200, 0.08, 0.46, seed=3)
+    p = str(tmp_path / "w.cnf")
+    dmm.write_cnf(f, p, planted=planted)
+    want = ("c [" + "".join(" %d" % (i + 1 if planted[i] > 0 else -(i + 1)) for i in range(300))
+            + " ]\np cnf 300 1200\n"
+            + "".join("".join("%d " % v for v in f.lits[f.clause_off[c]:f.clause_off[c + 1]]) + "0\n"
+                      for c in range(1200)))
+    assert open(p).read() == want
+    big, _ = dmm.generate_planted(100_000, 420_000, 0.08, 0.46, seed=4)  # several MB: many blocks
+    q = str(tmp_path / "big.cnf")
+    dmm.write_cnf(big, q)
+    g = dmm.read_cnf(q)
+    assert np.array_equal(g.lits, big.lits) and np.array_equal(g.clause_off, big.clause_off)
