@@ -74,9 +74,13 @@ def test_batch_tuning_does_not_change_results(fixtures):
             assert np.array_equal(a, c)
 
 
-def test_server_results_equal_alone(fixtures):
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_server_results_equal_alone(fixtures, prec):
+    """Requests arriving while others run; a formula may run alone for a while (the
+    single-formula form) and with others (the multi-formula form): every result equals
+    the formula's run alone."""
     items = mix(fixtures) + mix(fixtures)[:4]
-    srv = dmm.Server(budget_bytes=8 << 20, max_slots=5, steps_per_launch=16, precision="fp32")
+    srv = dmm.Server(budget_bytes=8 << 20, max_slots=5, steps_per_launch=16, precision=prec)
     tickets = {}
     pending = list(enumerate(items))
     done = {}
@@ -93,7 +97,7 @@ def test_server_results_equal_alone(fixtures):
         rounds += 1
         assert rounds < 10000
     for k, (form, x0) in enumerate(items):
-        r_a, post_a, _ = alone(form, x0, "fp32", 250)
+        r_a, post_a, _ = alone(form, x0, prec, 250)
         r_s = done[k]["result"]
         assert (r_s.status, r_s.steps, r_s.solved_step, r_s.t) == (
             r_a.status, r_a.steps, r_a.solved_step, r_a.t)
