@@ -111,12 +111,15 @@ def run_extras(device: int) -> dict:
         # set-up (formula upload, device CSR build, initial state) is inside both rates
         "solves_ratio_vs_plain": b["solves_per_s"] / max(p["solves_per_s"], 1e-9),
         "solves_ratio_vs_plain_run_only": b["solves_per_s_run"] / max(p["solves_per_s"], 1e-9),
-        "roofline": roofline(
+        "roofline": dict(roofline(
             sum((28 * it.formula.m + 8 * it.formula.n) * st for it, st in zip(items, b["steps"])),
             b["device_ms"], "k_inst (one block per formula, many steps per launch)",
             traffic=None,
             note="algorithmic bytes (28m + 8n per accepted step) of every formula's steps over "
-                 "the run's device time"),
+                 "the run's device time; traffic_over_algo: ncu DRAM bytes over algorithmic "
+                 "bytes of one captured launch (the 512 largest formulas' first 256 steps), "
+                 "read from the committed profile summary"),
+            traffic_over_algo=profiled_ratio("k_inst_c3.md")),
     }
     sv = w.make_items(300, 100, 100000, ratios=(4.3, 6.0, 8.0), seed=2)
     arr = w.poisson_times(len(sv), 200.0, seed=2)
@@ -233,6 +236,18 @@ KERNELS = {"staged": "k_staged (fused step, staged form)",
            "cooperative-single": "k_persist (fused step, single formula)",
            "cooperative": "k_persist (fused step)",
            "two-kernel": "k_clause + k_var", "one-block-per-formula": "k_inst"}
+
+
+def profiled_ratio(summary: str) -> float | None:
+    """DRAM bytes over algorithmic bytes of a captured launch, from a committed ncu summary
+    under profiles/ (its line `traffic_over_algo: X`); None when there is none."""
+    p = os.path.join(ROOT, "profiles", summary)
+    try:
+        with open(p) as f:
+            m = re.search(r"traffic_over_algo:\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
 
 
 def profiled_traffic(summary: str) -> float | None:
