@@ -224,6 +224,10 @@ static int persist_threads(dmm_precision prec) {
 }
 constexpr int kSlotPad = 8;             // entries past the last slot of vslot and u
 constexpr int kXpSmemMax = 220 * 1024;  // dynamic shared memory of the staged form, at most
+// ... and of its several-tiles-per-block form: beyond about 195 KB a block takes the largest
+// shared-memory carve-out, and the L1 left to the gathers shrinks (measured at 0.4-1.5 million
+// variables: every tiling above the cap ran 8-30 % slower than the best one below it)
+constexpr int kXpSmemMaxMT = 194 * 1024;
 constexpr int kXpMaxTiles = 1 << 14;    // clause or variable tiles of the staged form, at most
 constexpr int kMiscInts = 48;            // misc_d_: 192 bytes
 constexpr int kMiscLaunch = 16;          // misc_d_ index of the per-launch area (byte 64)
@@ -1153,7 +1157,7 @@ dmm_status Pack::prepare_xpose(int32_t idx, int TC, int TV, bool mt, bool* ok) {
   const int bk_cap = mt ? std::max(h[7], 8) : std::max(h[2], 8);
   const int smem = mt ? xp_layout_mt(sv_cap, st_cap, bk_cap, TV).total
                       : xp_layout(sv_cap, bk_cap, TV).total;
-  if (smem > kXpSmemMax) return DMM_OK;
+  if (smem > (mt ? kXpSmemMaxMT : kXpSmemMax)) return DMM_OK;
   if (occupancy_blocks(staged_fn(tun_.var_group, mt), kStagedThreads, smem) * sms_ != grid_p_)
     return DMM_OK;
   xsv_cap_ = sv_cap;
@@ -1217,13 +1221,13 @@ dmm_status Pack::prepare_xpose_mt(int32_t idx, bool* ok) {
       if (distinct > 30000 || stage > 60000 || bucket > 60000) continue;
       const double smem = 4.0 * std::max(distinct * 1.03 + stage, bucket) + 0.5 * bucket +
                           9.0 * TV + 4096;
-      if (smem > 0.97 * kXpSmemMax) continue;
+      if (smem > kXpSmemMaxMT + 7 * 1024) continue;  // the estimate runs up to ~6 KB high
       const double bytes = 4.0 * distinct * nct + 8.0 * 3.5 * nct * nvt;
       cands.push_back({TC, TV, 2.0 * (kc + kv) + bytes / 6.0e6});
     }
   }
   std::sort(cands.begin(), cands.end(), [](const Cand& a, const Cand& b) { return a.cost < b.cost; });
-  for (size_t k = 0; k < cands.size() && k < 4; k++) {
+  for (size_t k = 0; k < cands.size() && k < 8; k++) {
     DMM_TRY(set_tiles(idx, cands[k].TC, cands[k].TV));
     DMM_TRY(prepare_xpose(idx, cands[k].TC, cands[k].TV, true, ok));
     if (*ok) return DMM_OK;
