@@ -350,10 +350,9 @@ def test_fp64_energy_same_alone_and_in_a_batch_with_the_same_tiles(fixtures):
 
 def test_one_block_per_formula_with_contributions_in_global_memory():
     """One block per formula (launch mode 3) for formulas whose contributions do not fit in
-    the block's shared memory (more than 36,864 literal slots: slot-major in global memory)
-    and for ones that do (variable-major in shared memory), mixed in one batch: every
-    formula's state and report equal its run alone."""
-    sizes = [(5000, 40000), (8000, 20000), (1000, 8000), (4000, 12300), (4096, 12288)]
+    the block's shared memory (more than 32,256 literal slots: in global memory) and for ones
+    that do, mixed in one batch: every formula's state and report equal its run alone."""
+    sizes = [(5000, 40000), (8000, 20000), (1000, 8000), (4000, 10753), (4096, 10752)]
     forms = [dmm.generate_planted(n, m, 0.08, 0.46, seed=60 + k)[0] for k, (n, m) in enumerate(sizes)]
     x0s = [dmm.initial_state_uniform(f, 70 + k) for k, f in enumerate(forms)]
     b = dmm.Batch.for_formulas(forms, precision="fp32")
