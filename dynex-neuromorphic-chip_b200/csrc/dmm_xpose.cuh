@@ -175,6 +175,17 @@ __device__ __forceinline__ void prefetch_l2(const void* base, int64_t lo, int64_
   }
 }
 
+// Several-tiles form: each block's first kXpMetaTiles clause and variable tiles keep their
+// ranges and table offsets in shared memory for the whole launch, so a tile starts without a
+// dependent global load (tiles past those read them from global memory as they start).
+constexpr int kXpMetaTiles = 16;
+struct XpMetaC {
+  int begin, count, dbeg, dcnt, ubase, ulen;
+};
+struct XpMetaV {
+  int begin, count, bbeg, blen, jb;  // jb: CSR end before the tile
+};
+
 // The block's copy of the control state of the formula.
 struct StagedCtrl {
   int done, step, set, kcur, pending, best_loc;
@@ -236,6 +247,8 @@ __global__ void __launch_bounds__(NT, 1)
   __shared__ StagedCtrl lc;
   __shared__ Tile ctile, vtile;
   __shared__ int dbeg, dcnt, ubase, ulen, bbeg, blen;
+  __shared__ XpMetaC s_mc[MT ? kXpMetaTiles : 1];
+  __shared__ XpMetaV s_mv[MT ? kXpMetaTiles : 1];
   __shared__ double red[NT / 32];
   __shared__ int cnt[2][NT / 32];
   __shared__ int s_ok;
@@ -299,6 +312,28 @@ __global__ void __launch_bounds__(NT, 1)
     for (int w = tid; 4 * w < vtile.count; w += NT)
       cp_async4(s_unit + 4 * w, P.unit + I.var0 + vtile.begin + 4 * w);
   }
+  if constexpr (MT) {
+    if (tid < kXpMetaTiles) {
+      const int k = tid, ct = b + k * (int)gridDim.x, vt = ct;
+      if (ct < nct) {
+        XpMetaC& mc = s_mc[k];
+        mc.begin = P.ctiles[ct].begin;
+        mc.count = P.ctiles[ct].count;
+        mc.dbeg = __ldg(P.xdoff + 2 * ct);
+        mc.dcnt = __ldg(P.xdoff + 2 * ct + 1);
+        mc.ubase = __ldg(P.xubase + ct);
+        mc.ulen = __ldg(P.xubase + ct + 1) - mc.ubase;
+      }
+      if (vt < nvt) {
+        XpMetaV& mv = s_mv[k];
+        mv.begin = P.vtiles[vt].begin;
+        mv.count = P.vtiles[vt].count;
+        mv.bbeg = __ldg(P.xboff + vt);
+        mv.blen = __ldg(P.xboff + vt + 1) - mv.bbeg;
+        mv.jb = mv.begin > 0 ? __ldg(P.vend + I.var0 + mv.begin - 1) : 0;
+      }
+    }
+  }
   if (!MT && tid == 32 && lc.done == 0) {
     // the voltages of the first step: this block's share of them toward L2 (later steps
     // read the candidates the previous step wrote, still in L2)
@@ -327,12 +362,23 @@ __global__ void __launch_bounds__(NT, 1)
     // the block's clause tiles: b, b + grid, ... (one, b, without MT)
     for (int ct = b; ct < nct; ct += MT ? (int)gridDim.x : nct) {
       if constexpr (MT) {
+        const int k = (ct - b) / (int)gridDim.x;
         if (tid == 0) {
-          ctile = P.ctiles[ct];
-          dbeg = __ldg(P.xdoff + 2 * ct);
-          dcnt = __ldg(P.xdoff + 2 * ct + 1);
-          ubase = __ldg(P.xubase + ct);
-          ulen = __ldg(P.xubase + ct + 1) - ubase;
+          if (k < kXpMetaTiles) {
+            const XpMetaC& mc = s_mc[k];
+            ctile.begin = mc.begin;
+            ctile.count = mc.count;
+            dbeg = mc.dbeg;
+            dcnt = mc.dcnt;
+            ubase = mc.ubase;
+            ulen = mc.ulen;
+          } else {
+            ctile = P.ctiles[ct];
+            dbeg = __ldg(P.xdoff + 2 * ct);
+            dcnt = __ldg(P.xdoff + 2 * ct + 1);
+            ubase = __ldg(P.xubase + ct);
+            ulen = __ldg(P.xubase + ct + 1) - ubase;
+          }
         }
         __syncthreads();
         // one warp asks L2 for the block's next clause tile (its variable list, local
@@ -583,14 +629,24 @@ __global__ void __launch_bounds__(NT, 1)
     // the block's variable tiles: b, b + grid, ... (one, b, without MT)
     for (int vt = b; vt < nvt; vt += MT ? (int)gridDim.x : nvt) {
       if constexpr (MT) {
+        const int k = (vt - b) / (int)gridDim.x;
         if (tid == 0) {
-          vtile = P.vtiles[vt];
-          bbeg = __ldg(P.xboff + vt);
-          blen = __ldg(P.xboff + vt + 1) - bbeg;
+          if (k < kXpMetaTiles) {
+            const XpMetaV& mv = s_mv[k];
+            vtile.begin = mv.begin;
+            vtile.count = mv.count;
+            bbeg = mv.bbeg;
+            blen = mv.blen;
+          } else {
+            vtile = P.vtiles[vt];
+            bbeg = __ldg(P.xboff + vt);
+            blen = __ldg(P.xboff + vt + 1) - bbeg;
+          }
         }
         __syncthreads();
         const int32_t* vend = P.vend + I.var0;
-        const int jb = vtile.begin > 0 ? __ldg(vend + vtile.begin - 1) : 0;
+        const int jb = k < kXpMetaTiles ? s_mv[k].jb
+                                        : vtile.begin > 0 ? __ldg(vend + vtile.begin - 1) : 0;
         for (int g = tid; g < blen / 8; g += NT) s_src8[g] = __ldg(P.xsrc8 + bbeg / 8 + g);
         for (int i = tid; i <= vtile.count; i += NT)
           s_vend[i] = i == 0 ? 0 : __ldg(vend + vtile.begin + i - 1) - jb;

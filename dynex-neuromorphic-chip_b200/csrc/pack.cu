@@ -227,7 +227,7 @@ constexpr int kXpSmemMax = 220 * 1024;  // dynamic shared memory of the staged f
 // ... and of its several-tiles-per-block form: beyond about 195 KB a block takes the largest
 // shared-memory carve-out, and the L1 left to the gathers shrinks (measured at 0.4-1.5 million
 // variables: every tiling above the cap ran 8-30 % slower than the best one below it)
-constexpr int kXpSmemMaxMT = 194 * 1024;
+constexpr int kXpSmemMaxMT = 193 * 1024;  // with the form's ~1.4 KB of static shared memory
 constexpr int kXpMaxTiles = 1 << 14;    // clause or variable tiles of the staged form, at most
 constexpr int kMiscInts = 48;            // misc_d_: 192 bytes
 constexpr int kMiscLaunch = 16;          // misc_d_ index of the per-launch area (byte 64)
